@@ -1,0 +1,134 @@
+/*
+ * psp_b200 — C ABI of the B200-native sweeping-preconditioned Helmholtz solver.
+ *
+ * Plain pointers and sizes only; every call returns a psp_cu_status and never
+ * throws.  The C++ surface (include/psp/psp.hpp) and the Python binding
+ * (psp_b200/__init__.py) are thin layers over these entry points.
+ *
+ * Grids are natural order (x fastest, then y, then z) and complex grids carry
+ * the k right-hand sides interleaved per point, i.e. the buffer layout of a
+ * one-process psp::DistUniformGrid<Complex<double>> with numScalars = k
+ * (PSP include/psp/dist_uniform_grid.hpp:292-342).  Complex numbers are two
+ * doubles (re, im).
+ *
+ * Threading: a handle is thread-compatible, not thread-safe; it owns one CUDA
+ * stream and all of its device memory.  The caller owns every buffer it
+ * passes in.
+ */
+#ifndef PSP_B200_H
+#define PSP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PSP_CU_OK = 0,
+    PSP_CU_LOGIC_ERROR = 1,     /* std::logic_error in the reference */
+    PSP_CU_RUNTIME_ERROR = 2,   /* std::runtime_error in the reference */
+    PSP_CU_CUDA_ERROR = 3,
+    PSP_CU_OUT_OF_MEMORY = 4,
+    PSP_CU_NOT_INITIALIZED = 5,
+    PSP_CU_NO_DEVICE = 6
+} psp_cu_status;
+
+typedef enum { PSP_CU_PML = 0, PSP_CU_DIRICHLET = 1 } psp_cu_boundary;
+
+/* psp::PanelScheme (include/psp/dist_helmholtz.hpp:14-19). */
+typedef enum { PSP_CU_LDL_1D = 0, PSP_CU_LDL_SELINV_1D = 1 } psp_cu_panel_scheme;
+
+/* Arithmetic of the panel fronts and sweeps; GMRES, the residual matvec and
+ * the Arnoldi/Givens work are FP64 in both modes. */
+typedef enum { PSP_CU_FP64 = 0, PSP_CU_MIXED = 1 } psp_cu_precision;
+
+/* psp::Discretization<double> (include/psp/discretization.hpp:36-110). */
+typedef struct {
+    double omega;
+    int nx, ny, nz;
+    double wx, wy, wz;
+    int frontBC, rightBC, backBC, leftBC, topBC; /* psp_cu_boundary */
+    int bx, by, bz;
+    double sigmax, sigmay, sigmaz;
+} psp_cu_disc;
+
+typedef struct {
+    int iterations;            /* GMRES inner steps taken */
+    int converged;
+    int lucky_breakdown;       /* B then holds the right-hand sides (solve.hpp:405-414) */
+    double final_max_rel_resid;
+    double solve_seconds;
+    double precondition_seconds;
+    double matvec_seconds;
+    double arnoldi_seconds;
+    int num_preconditions;
+} psp_cu_stats;
+
+typedef struct psp_cu_handle psp_cu_handle;
+
+/* Last error message of the calling thread. */
+const char* psp_cu_last_error(void);
+
+/* DistHelmholtz<double>(disc, comm, damping, numPlanesPerPanel, cutoff)
+ * (include/psp/dist_helmholtz/main.hpp:12-436).  Throws nothing; a shallow
+ * domain (main.hpp:38-41) returns PSP_CU_LOGIC_ERROR. */
+int psp_cu_create(const psp_cu_disc* disc, double damping, int planes_per_panel, int cutoff, int device,
+                  psp_cu_handle** out);
+
+/* ~DistHelmholtz. */
+void psp_cu_destroy(psp_cu_handle* h);
+
+/* DistHelmholtz::Initialize(velocity, panelScheme)
+ * (include/psp/dist_helmholtz/initialize_finalize.hpp:12-377); velocity is a
+ * host array of nx*ny*nz doubles in natural order. */
+int psp_cu_initialize(psp_cu_handle* h, const double* velocity, int panel_scheme, int precision);
+
+/* Same with the velocity already in device memory of the handle's GPU. */
+int psp_cu_initialize_device(psp_cu_handle* h, const double* d_velocity, int panel_scheme, int precision);
+
+/* DistHelmholtz::Solve(B, m, relTol) (include/psp/dist_helmholtz/solve.hpp:12-56):
+ * B is a host grid of nx*ny*nz*k complex values, overwritten by the solution. */
+int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_cu_stats* stats);
+
+/* The same on a device grid owned by the caller. */
+int psp_cu_solve_device(psp_cu_handle* h, double* d_B, int k, int m, double rel_tol, psp_cu_stats* stats);
+
+/* DistHelmholtz::Finalize() (initialize_finalize.hpp:379-396): frees the factors. */
+int psp_cu_finalize(psp_cu_handle* h);
+
+/* B := A B with the global operator (Multiply, solve.hpp:613-679); host grid. */
+int psp_cu_multiply(psp_cu_handle* h, double* B, int k);
+
+/* B := M^{-1} B, one application of the sweeping preconditioner
+ * (Precondition, solve.hpp:681-734); host grid. */
+int psp_cu_precondition(psp_cu_handle* h, double* B, int k);
+
+/* Device-grid variants of the two calls above. */
+int psp_cu_multiply_device(psp_cu_handle* h, double* d_B, int k);
+int psp_cu_precondition_device(psp_cu_handle* h, double* d_B, int k);
+
+/* B := T_p B on panel p only (SolvePanel, solve.hpp:736-882); host grid. */
+int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel);
+
+/* Cap on GMRES inner steps (0 = none, the reference behaviour). */
+int psp_cu_set_max_iterations(psp_cu_handle* h, int max_iterations);
+
+/* Panel geometry: number of panels and, if info != NULL, 4 ints per panel
+ * (lowest v, depth, padding, class) as in main.hpp:728-821. */
+int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info);
+
+/* Seconds spent in the last Initialize and bytes of stored panel factors. */
+int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* factor_bytes);
+
+/* Host-only symbolic analysis (no GPU needed): the elimination tree of panel
+ * class cls (0 bottom/full inner, 1 leftover, 2 top; main.hpp:705-726) as
+ * 4 ints per node (ND offset, pivot count, update count, parent) in postorder,
+ * and optionally its ND -> panel-natural map (nx*ny*vSize ints).  Pass
+ * info = NULL to query num_nodes and vsize. */
+int psp_cu_analyze_class(const psp_cu_disc* disc, int planes_per_panel, int cutoff, int cls, int* num_nodes,
+                         int* vsize, int* info, int* nd_to_nat);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSP_B200_H */

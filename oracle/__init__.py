@@ -1,0 +1,185 @@
+"""ORACLE — test infrastructure only (the checker, never the product).
+
+ctypes front-end for ``liboracle.so``, the FP64 CPU restatement of PSP's
+sweeping-preconditioned Helmholtz solve built from ``psp_oracle.cpp``.
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
+this module.
+
+Grids are numpy arrays in natural order (x fastest, then y, then z), complex
+grids carry the ``k`` right-hand sides interleaved per point, i.e. shape
+``(nz, ny, nx, k)`` -- the layout of a one-process ``DistUniformGrid`` with
+``numScalars = k`` (dist_uniform_grid.hpp:292-342).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+PML, DIRICHLET = 0, 1
+
+
+class _Disc(ctypes.Structure):
+    _fields_ = [
+        ("omega", ctypes.c_double),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("wx", ctypes.c_double), ("wy", ctypes.c_double), ("wz", ctypes.c_double),
+        ("frontBC", ctypes.c_int), ("rightBC", ctypes.c_int), ("backBC", ctypes.c_int),
+        ("leftBC", ctypes.c_int), ("topBC", ctypes.c_int),
+        ("bx", ctypes.c_int), ("by", ctypes.c_int), ("bz", ctypes.c_int),
+        ("sigmax", ctypes.c_double), ("sigmay", ctypes.c_double), ("sigmaz", ctypes.c_double),
+    ]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int), ("converged", ctypes.c_int),
+        ("lucky_breakdown", ctypes.c_int), ("final_max_rel_resid", ctypes.c_double),
+        ("setup_seconds", ctypes.c_double), ("solve_seconds", ctypes.c_double),
+    ]
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.oracle_create.argtypes = [ctypes.POINTER(_Disc), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p)]
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_last_error.restype = ctypes.c_char_p
+        L.oracle_geometry.argtypes = [vp, ip, ip]
+        L.oracle_nd_to_natural.argtypes = [vp, ip]
+        L.oracle_tree.argtypes = [vp, ctypes.c_int, ip, ip]
+        L.oracle_initialize.argtypes = [vp, dp]
+        L.oracle_global_operator.argtypes = [vp, ip, ip, ip, dp]
+        L.oracle_multiply.argtypes = [vp, dp, ctypes.c_int]
+        L.oracle_precondition.argtypes = [vp, dp, ctypes.c_int]
+        L.oracle_solve_panel.argtypes = [vp, dp, ctypes.c_int, ctypes.c_int]
+        L.oracle_solve.argtypes = [vp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                   ctypes.POINTER(_Stats), dp, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a, ctype=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def make_disc(omega, nx, ny, nz, wx, wy, wz, bcs=(PML,) * 5, pml=(5, 5, 5), sigma=None):
+    """Discretization<R> (discretization.hpp:36-110). ``sigma=None`` uses
+    the reference default 1.2*max width (discretization.hpp:59-62)."""
+    d = _Disc()
+    d.omega = omega
+    d.nx, d.ny, d.nz = nx, ny, nz
+    d.wx, d.wy, d.wz = wx, wy, wz
+    d.frontBC, d.rightBC, d.backBC, d.leftBC, d.topBC = bcs
+    d.bx, d.by, d.bz = pml
+    s = 1.2 * max(wx, wy, wz) if sigma is None else sigma
+    d.sigmax = d.sigmay = d.sigmaz = s
+    return d
+
+
+class Oracle:
+    """FP64 CPU DistHelmholtz restatement (one process)."""
+
+    def __init__(self, disc, damping=7.0, planes_per_panel=4, cutoff=12):
+        self.disc = disc
+        h = ctypes.c_void_p()
+        if lib().oracle_create(ctypes.byref(disc), damping, planes_per_panel, cutoff, ctypes.byref(h)):
+            raise ValueError(lib().oracle_last_error().decode())
+        self._h = h
+        self.shape = (disc.nz, disc.ny, disc.nx)
+        self.N = disc.nx * disc.ny * disc.nz
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().oracle_destroy(self._h)
+            self._h = None
+
+    def geometry(self):
+        n = ctypes.c_int()
+        lib().oracle_geometry(self._h, ctypes.byref(n), None)
+        info = np.zeros(4 * n.value, dtype=np.int32)
+        lib().oracle_geometry(self._h, ctypes.byref(n), _ptr(info, ctypes.c_int))
+        return info.reshape(n.value, 4)  # (vLow, depth, padding, class)
+
+    def nd_to_natural(self):
+        out = np.zeros(self.N, dtype=np.int32)
+        lib().oracle_nd_to_natural(self._h, _ptr(out, ctypes.c_int))
+        return out
+
+    def tree(self, cls):
+        n = ctypes.c_int()
+        lib().oracle_tree(self._h, cls, ctypes.byref(n), None)
+        info = np.zeros(4 * n.value, dtype=np.int32)
+        lib().oracle_tree(self._h, cls, ctypes.byref(n), _ptr(info, ctypes.c_int))
+        return info.reshape(n.value, 4)  # (off, size, lowerSize, parent)
+
+    def initialize(self, velocity):
+        v = np.ascontiguousarray(velocity, dtype=np.float64)
+        assert v.size == self.N
+        if lib().oracle_initialize(self._h, _ptr(v)):
+            raise RuntimeError(lib().oracle_last_error().decode())
+
+    def global_operator_natural(self):
+        """The global operator as a scipy CSR matrix in natural ordering."""
+        import scipy.sparse as sp
+        nnz = ctypes.c_int()
+        lib().oracle_global_operator(self._h, ctypes.byref(nnz), None, None, None)
+        rp = np.zeros(self.N + 1, dtype=np.int32)
+        cols = np.zeros(nnz.value, dtype=np.int32)
+        vals = np.zeros(2 * nnz.value, dtype=np.float64)
+        lib().oracle_global_operator(self._h, ctypes.byref(nnz), _ptr(rp, ctypes.c_int),
+                                     _ptr(cols, ctypes.c_int), _ptr(vals))
+        A_nd = sp.csr_matrix((vals.view(np.complex128), cols, rp), shape=(self.N, self.N))
+        perm = self.nd_to_natural()
+        P = sp.csr_matrix((np.ones(self.N), (perm, np.arange(self.N))), shape=(self.N, self.N))
+        return (P @ A_nd @ P.T).tocsr()
+
+    def _grid_call(self, fn, B, *extra):
+        X = np.ascontiguousarray(B, dtype=np.complex128).copy()
+        k = X.size // self.N
+        if fn(self._h, _ptr(X.view(np.float64)), k, *extra):
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return X
+
+    def multiply(self, B):
+        return self._grid_call(lib().oracle_multiply, B)
+
+    def precondition(self, B):
+        return self._grid_call(lib().oracle_precondition, B)
+
+    def solve_panel(self, B, p):
+        return self._grid_call(lib().oracle_solve_panel, B, p)
+
+    def solve(self, B, m=20, rel_tol=1e-4, max_its=0, history=64):
+        """Returns (X, stats dict)."""
+        X = np.ascontiguousarray(B, dtype=np.complex128).copy()
+        k = X.size // self.N
+        st = _Stats()
+        hist = np.zeros(max(history, 1), dtype=np.float64)
+        if lib().oracle_solve(self._h, _ptr(X.view(np.float64)), k, m, rel_tol, max_its,
+                              ctypes.byref(st), _ptr(hist), history):
+            raise RuntimeError(lib().oracle_last_error().decode())
+        stats = dict(iterations=st.iterations, converged=bool(st.converged),
+                     lucky_breakdown=bool(st.lucky_breakdown),
+                     final_max_rel_resid=st.final_max_rel_resid,
+                     history=hist[:min(st.iterations, history)].copy())
+        return X, stats
+
+
+def num_threads():
+    lib().oracle_num_threads.restype = ctypes.c_int
+    return lib().oracle_num_threads()

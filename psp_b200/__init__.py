@@ -1,0 +1,346 @@
+"""psp_b200 — B200-native drop-in for PSP's sweeping-preconditioned Helmholtz solve.
+
+Python mirror of the reference's C++ surface over the C ABI of
+``libpsp_b200.so`` (include/psp_b200.h):
+
+* :class:`Discretization` — ``psp::Discretization<R>`` (discretization.hpp:36-110)
+* :class:`DistUniformGrid` — ``psp::DistUniformGrid<F>`` for one process
+  (dist_uniform_grid.hpp:48-145), natural order with ``numScalars`` entries
+  interleaved per point
+* :class:`DistHelmholtz` — ``psp::DistHelmholtz<R>`` (dist_helmholtz.hpp:21-287):
+  ``Initialize(velocity, panelScheme)``, ``Solve(B, m, relTol)`` (alias
+  ``SolveWithGMRES``) and ``Finalize()``
+
+The compute path is the CUDA library; there is no CPU fallback: importing
+works without a GPU, but every compute call fails loudly when the library or
+the device is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpsp_b200.so")
+
+PML, DIRICHLET = 0, 1
+CLIQUE_LDL_1D, CLIQUE_LDL_SELINV_1D = 0, 1
+FP64, MIXED = 0, 1
+XYZ, XZY, YXZ, YZX, ZXY, ZYX = range(6)
+
+_STATUS = {0: "ok", 1: "logic error", 2: "runtime error", 3: "CUDA error", 4: "out of memory",
+           5: "not initialized", 6: "no CUDA device"}
+
+
+class LogicError(ValueError):
+    """``std::logic_error`` of the reference (bad arguments, shallow domain, ...)."""
+
+
+class PspRuntimeError(RuntimeError):
+    """``std::runtime_error`` of the reference (NaN in GMRES, zero pivot, ...)."""
+
+
+class CudaError(RuntimeError):
+    """A CUDA failure (including out-of-memory and no device)."""
+
+
+class _Disc(ctypes.Structure):
+    _fields_ = [
+        ("omega", ctypes.c_double),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("wx", ctypes.c_double), ("wy", ctypes.c_double), ("wz", ctypes.c_double),
+        ("frontBC", ctypes.c_int), ("rightBC", ctypes.c_int), ("backBC", ctypes.c_int),
+        ("leftBC", ctypes.c_int), ("topBC", ctypes.c_int),
+        ("bx", ctypes.c_int), ("by", ctypes.c_int), ("bz", ctypes.c_int),
+        ("sigmax", ctypes.c_double), ("sigmay", ctypes.c_double), ("sigmaz", ctypes.c_double),
+    ]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("lucky_breakdown", ctypes.c_int),
+        ("final_max_rel_resid", ctypes.c_double), ("solve_seconds", ctypes.c_double),
+        ("precondition_seconds", ctypes.c_double), ("matvec_seconds", ctypes.c_double),
+        ("arnoldi_seconds", ctypes.c_double), ("num_preconditions", ctypes.c_int),
+    ]
+
+
+C_ABI_SYMBOLS = [
+    "psp_cu_last_error", "psp_cu_create", "psp_cu_destroy", "psp_cu_initialize", "psp_cu_initialize_device",
+    "psp_cu_solve", "psp_cu_solve_device", "psp_cu_finalize", "psp_cu_multiply", "psp_cu_precondition",
+    "psp_cu_multiply_device", "psp_cu_precondition_device", "psp_cu_solve_panel", "psp_cu_set_max_iterations",
+    "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class",
+]
+
+_lib = None
+
+
+def lib():
+    """The loaded C ABI library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libpsp_b200.so is missing: run `python -m psp_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.psp_cu_last_error.restype = ctypes.c_char_p
+        L.psp_cu_create.argtypes = [ctypes.POINTER(_Disc), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.POINTER(vp)]
+        L.psp_cu_destroy.argtypes = [vp]
+        L.psp_cu_destroy.restype = None
+        L.psp_cu_initialize.argtypes = [vp, dp, ctypes.c_int, ctypes.c_int]
+        L.psp_cu_initialize_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int]
+        L.psp_cu_solve.argtypes = [vp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(_Stats)]
+        L.psp_cu_solve_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                          ctypes.POINTER(_Stats)]
+        L.psp_cu_finalize.argtypes = [vp]
+        L.psp_cu_multiply.argtypes = [vp, dp, ctypes.c_int]
+        L.psp_cu_precondition.argtypes = [vp, dp, ctypes.c_int]
+        L.psp_cu_multiply_device.argtypes = [vp, vp, ctypes.c_int]
+        L.psp_cu_precondition_device.argtypes = [vp, vp, ctypes.c_int]
+        L.psp_cu_solve_panel.argtypes = [vp, dp, ctypes.c_int, ctypes.c_int]
+        L.psp_cu_set_max_iterations.argtypes = [vp, ctypes.c_int]
+        L.psp_cu_geometry.argtypes = [vp, ip, ip]
+        L.psp_cu_setup_info.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
+        L.psp_cu_analyze_class.argtypes = [ctypes.POINTER(_Disc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ip, ip, ip, ip]
+        _lib = L
+    return _lib
+
+
+def _check(code):
+    if code == 0:
+        return
+    msg = lib().psp_cu_last_error().decode()
+    if code == 1:
+        raise LogicError(msg)
+    if code in (2, 5):
+        raise PspRuntimeError(msg)
+    raise CudaError("%s: %s" % (_STATUS.get(code, code), msg))
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Discretization:
+    """``psp::Discretization<R>`` (discretization.hpp:36-110).
+
+    Mirrors the four constructors: ``Discretization(omega, nx, ny, nz, wx, wy, wz)``
+    plus optional boundary conditions ``bcs=(front, right, back, left, top)``
+    and either ``pml=(bx, by, bz)`` (sigma = 1.2*max width) or
+    ``pml=size, sigma=value``.  Widths are those of the PML-padded box.
+    """
+
+    def __init__(self, omega, nx, ny, nz, wx, wy, wz, bcs=(PML,) * 5, pml=(5, 5, 5), sigma=None):
+        self.omega = float(omega)
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.wx, self.wy, self.wz = float(wx), float(wy), float(wz)
+        self.frontBC, self.rightBC, self.backBC, self.leftBC, self.topBC = bcs
+        if np.isscalar(pml):
+            pml = (pml, pml, pml)
+        self.bx, self.by, self.bz = (int(v) for v in pml)
+        s = 1.2 * max(self.wx, self.wy, self.wz) if sigma is None else float(sigma)
+        self.sigmax = self.sigmay = self.sigmaz = s
+
+    def _c(self):
+        d = _Disc()
+        for name, _ in _Disc._fields_:
+            setattr(d, name, getattr(self, name))
+        return d
+
+
+class DistUniformGrid:
+    """``psp::DistUniformGrid<F>`` on one process (dist_uniform_grid.hpp:48-145).
+
+    ``data`` has shape (nz, ny, nx, numScalars) in XYZ order -- exactly the
+    reference's local buffer with px = py = pz = 1.  Other storage orders are
+    accepted by :meth:`from_order` and converted to XYZ.
+    """
+
+    def __init__(self, nx, ny, nz, numScalars=1, dtype=np.complex128, data=None):
+        self.nx, self.ny, self.nz, self.numScalars = nx, ny, nz, numScalars
+        if data is None:
+            data = np.zeros((nz, ny, nx, numScalars), dtype=dtype)
+        self.data = np.ascontiguousarray(np.asarray(data, dtype=dtype).reshape(nz, ny, nx, numScalars))
+
+    def XSize(self): return self.nx
+    def YSize(self): return self.ny
+    def ZSize(self): return self.nz
+    def NumScalars(self): return self.numScalars
+    def XShift(self): return 0
+    def YShift(self): return 0
+    def ZShift(self): return 0
+    def XStride(self): return 1
+    def YStride(self): return 1
+    def ZStride(self): return 1
+    def XLocalSize(self): return self.nx
+    def YLocalSize(self): return self.ny
+    def ZLocalSize(self): return self.nz
+    def OwningProcess(self, *args): return 0
+
+    def NaturalIndex(self, x, y, z):
+        return x + y * self.nx + z * self.nx * self.ny
+
+    def LocalIndex(self, x, y, z):
+        """Offset of point (x, y, z) in the flat buffer (dist_uniform_grid.hpp:316-342)."""
+        return self.NaturalIndex(x, y, z) * self.numScalars
+
+    def Buffer(self):
+        return self.data.reshape(-1)
+
+    @classmethod
+    def from_order(cls, buf, nx, ny, nz, numScalars, order, dtype=np.complex128):
+        """Build an XYZ grid from a flat buffer stored in one of the six
+        GridDataOrder layouts (dist_uniform_grid.hpp:316-339)."""
+        a = np.asarray(buf, dtype=dtype).reshape(-1, numScalars)
+        dims = {XYZ: (nz, ny, nx), XZY: (ny, nz, nx), YXZ: (nz, nx, ny), YZX: (nx, nz, ny),
+                ZXY: (ny, nx, nz), ZYX: (nx, ny, nz)}[order]
+        # transpose taking the stored (slowest..fastest) axes to (z, y, x)
+        perm = {XYZ: (0, 1, 2), XZY: (1, 0, 2), YXZ: (0, 2, 1), YZX: (1, 2, 0),
+                ZXY: (2, 0, 1), ZYX: (2, 1, 0)}[order]
+        v = np.transpose(a.reshape(*dims, numScalars), perm + (3,))
+        return cls(nx, ny, nz, numScalars, dtype, v)
+
+
+def analyze_class(disc, planes_per_panel=4, cutoff=12, cls=0):
+    """Host-only symbolic analysis of one panel class: returns (info, ndToNat)
+    with info rows (ND offset, pivot count, update count, parent)."""
+    d = disc._c()
+    n = ctypes.c_int()
+    vs = ctypes.c_int()
+    _check(lib().psp_cu_analyze_class(ctypes.byref(d), planes_per_panel, cutoff, cls, ctypes.byref(n),
+                                      ctypes.byref(vs), None, None))
+    info = np.zeros(4 * n.value, dtype=np.int32)
+    nd = np.zeros(disc.nx * disc.ny * vs.value, dtype=np.int32)
+    _check(lib().psp_cu_analyze_class(ctypes.byref(d), planes_per_panel, cutoff, cls, ctypes.byref(n),
+                                      ctypes.byref(vs), _iptr(info), _iptr(nd)))
+    return info.reshape(n.value, 4), nd
+
+
+class DistHelmholtz:
+    """``psp::DistHelmholtz<double>`` on one B200 (dist_helmholtz.hpp:21-287).
+
+    ``DistHelmholtz(disc, damping=7.0, numPlanesPerPanel=4, cutoff=12)``;
+    the MPI communicator of the reference is replaced by a CUDA device index.
+    """
+
+    def __init__(self, disc, damping=7.0, numPlanesPerPanel=4, cutoff=12, device=0):
+        self.disc = disc
+        self._h = None
+        h = ctypes.c_void_p()
+        self._d = disc._c()
+        _check(lib().psp_cu_create(ctypes.byref(self._d), float(damping), int(numPlanesPerPanel), int(cutoff),
+                                   int(device), ctypes.byref(h)))
+        self._h = h
+        self.N = disc.nx * disc.ny * disc.nz
+        self.last_stats = None
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().psp_cu_destroy(self._h)
+            self._h = None
+
+    def geometry(self):
+        n = ctypes.c_int()
+        _check(lib().psp_cu_geometry(self._h, ctypes.byref(n), None))
+        info = np.zeros(4 * n.value, dtype=np.int32)
+        _check(lib().psp_cu_geometry(self._h, ctypes.byref(n), _iptr(info)))
+        return info.reshape(n.value, 4)
+
+    def Initialize(self, velocity, panelScheme=CLIQUE_LDL_SELINV_1D, precision=FP64):
+        """Assemble and factor every panel (initialize_finalize.hpp:12-377).
+        ``velocity`` is a DistUniformGrid, a numpy array (natural order) or a
+        CUDA torch tensor of float64."""
+        if isinstance(velocity, DistUniformGrid):
+            if (velocity.nx, velocity.ny, velocity.nz) != (self.disc.nx, self.disc.ny, self.disc.nz):
+                raise LogicError("Velocity grid is incorrect")
+            if velocity.numScalars != 1:
+                raise LogicError("Velocity grid should have one entry per point")
+            velocity = velocity.data
+        if _is_cuda_tensor(velocity):
+            if velocity.numel() != self.N:
+                raise LogicError("Velocity grid is incorrect")
+            v = velocity.contiguous()
+            _check(lib().psp_cu_initialize_device(self._h, ctypes.c_void_p(v.data_ptr()), panelScheme, precision))
+            return
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        if v.size != self.N:
+            raise LogicError("Velocity grid is incorrect")
+        _check(lib().psp_cu_initialize(self._h, _dptr(v), panelScheme, precision))
+
+    def Solve(self, B, m=20, relTol=1e-4, viewIterates=False):
+        """Solve in place (solve.hpp:12-56).  ``B`` is a complex DistUniformGrid
+        whose numScalars right-hand sides are replaced by the solutions, or a
+        CUDA complex128 torch tensor of nx*ny*nz*k entries."""
+        if _is_cuda_tensor(B):
+            k = B.numel() // self.N
+            st = _Stats()
+            _check(lib().psp_cu_solve_device(self._h, ctypes.c_void_p(B.data_ptr()), k, m, relTol,
+                                             ctypes.byref(st)))
+            self.last_stats = _stats_dict(st)
+            return self.last_stats
+        grid = B if isinstance(B, DistUniformGrid) else None
+        arr = grid.data if grid is not None else B
+        if arr.dtype != np.complex128 or not arr.flags["C_CONTIGUOUS"]:
+            raise LogicError("B must be a C-contiguous complex128 grid")
+        k = arr.size // self.N
+        if k * self.N != arr.size:
+            raise LogicError("B does not match the grid")
+        st = _Stats()
+        _check(lib().psp_cu_solve(self._h, _dptr(arr.view(np.float64)), k, m, relTol, ctypes.byref(st)))
+        self.last_stats = _stats_dict(st)
+        return self.last_stats
+
+    SolveWithGMRES = Solve
+
+    def Finalize(self):
+        _check(lib().psp_cu_finalize(self._h))
+
+    def set_max_iterations(self, n):
+        _check(lib().psp_cu_set_max_iterations(self._h, int(n)))
+
+    def setup_info(self):
+        s = ctypes.c_double()
+        b = ctypes.c_longlong()
+        _check(lib().psp_cu_setup_info(self._h, ctypes.byref(s), ctypes.byref(b)))
+        return s.value, b.value
+
+    def _grid_op(self, fn, B, *extra):
+        X = np.ascontiguousarray(B, dtype=np.complex128).copy()
+        k = X.size // self.N
+        _check(fn(self._h, _dptr(X.view(np.float64)), k, *extra))
+        return X
+
+    def multiply(self, B):
+        """B := A B (Multiply, solve.hpp:613-679) on a copy."""
+        return self._grid_op(lib().psp_cu_multiply, B)
+
+    def precondition(self, B):
+        """B := M^{-1} B (Precondition, solve.hpp:681-734) on a copy."""
+        return self._grid_op(lib().psp_cu_precondition, B)
+
+    def solve_panel(self, B, p):
+        """B := T_p B on panel p only (SolvePanel, solve.hpp:736-882) on a copy."""
+        return self._grid_op(lib().psp_cu_solve_panel, B, int(p))
+
+    def multiply_device(self, B):
+        _check(lib().psp_cu_multiply_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+
+    def precondition_device(self, B):
+        _check(lib().psp_cu_precondition_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+
+
+def _stats_dict(st):
+    return dict(iterations=st.iterations, converged=bool(st.converged), lucky_breakdown=bool(st.lucky_breakdown),
+                final_max_rel_resid=st.final_max_rel_resid, solve_seconds=st.solve_seconds,
+                precondition_seconds=st.precondition_seconds, matvec_seconds=st.matvec_seconds,
+                arnoldi_seconds=st.arnoldi_seconds, num_preconditions=st.num_preconditions)
+
+
+def _is_cuda_tensor(x):
+    return getattr(x, "is_cuda", False) and hasattr(x, "data_ptr")

@@ -1,0 +1,227 @@
+// C ABI over psp_b200::Helmholtz: converts exceptions into status codes.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "../../include/psp_b200.h"
+#include "solver.hpp"
+
+using psp_b200::Helmholtz;
+using psp_b200::PspError;
+
+struct psp_cu_handle {
+    Helmholtz* solver;
+};
+
+namespace {
+
+thread_local std::string g_lastError;
+
+template <typename F>
+int Guard(F&& fn) {
+    try {
+        fn();
+        g_lastError.clear();
+        return PSP_CU_OK;
+    } catch (const PspError& e) {
+        g_lastError = e.what();
+        return e.code;
+    } catch (const std::bad_alloc& e) {
+        g_lastError = "host allocation failed";
+        return PSP_CU_OUT_OF_MEMORY;
+    } catch (const std::logic_error& e) {
+        g_lastError = e.what();
+        return PSP_CU_LOGIC_ERROR;
+    } catch (const std::exception& e) {
+        g_lastError = e.what();
+        return PSP_CU_RUNTIME_ERROR;
+    }
+}
+
+int CheckHandle(const psp_cu_handle* h) {
+    if (!h || !h->solver) {
+        g_lastError = "null handle";
+        return PSP_CU_LOGIC_ERROR;
+    }
+    return PSP_CU_OK;
+}
+
+void FillStats(const psp_b200::SolveStats& s, psp_cu_stats* out) {
+    if (!out) return;
+    out->iterations = s.iterations;
+    out->converged = s.converged;
+    out->lucky_breakdown = s.luckyBreakdown;
+    out->final_max_rel_resid = s.finalMaxRelResid;
+    out->solve_seconds = s.seconds;
+    out->precondition_seconds = s.precondSeconds;
+    out->matvec_seconds = s.matvecSeconds;
+    out->arnoldi_seconds = s.arnoldiSeconds;
+    out->num_preconditions = s.numPreconditions;
+}
+
+// Runs fn on a device copy of the host grid B and copies the result back.
+template <typename F>
+void OnDeviceCopy(Helmholtz* s, double* B, int k, F&& fn) {
+    if (!B) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
+    if (k < 1) throw PspError(PSP_CU_LOGIC_ERROR, "need at least one right-hand side");
+    const size_t bytes = (size_t)s->NumUnknowns() * k * 2 * sizeof(double);
+    psp_b200::DeviceBuffer d;
+    d.Allocate(bytes);
+    CUDA_CHECK(cudaMemcpyAsync(d.p, B, bytes, cudaMemcpyHostToDevice, s->stream()));
+    fn(d.as<psp_b200::z64>());
+    CUDA_CHECK(cudaMemcpyAsync(B, d.p, bytes, cudaMemcpyDeviceToHost, s->stream()));
+    CUDA_CHECK(cudaStreamSynchronize(s->stream()));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* psp_cu_last_error(void) { return g_lastError.c_str(); }
+
+int psp_cu_create(const psp_cu_disc* disc, double damping, int planes_per_panel, int cutoff, int device,
+                  psp_cu_handle** out) {
+    if (!disc || !out) {
+        g_lastError = "null argument";
+        return PSP_CU_LOGIC_ERROR;
+    }
+    *out = nullptr;
+    return Guard([&] {
+        psp_b200::DiscParams d;
+        static_assert(sizeof(psp_b200::DiscParams) == sizeof(psp_cu_disc), "disc layout");
+        std::memcpy(&d, disc, sizeof(d));
+        Helmholtz* s = new Helmholtz(d, damping, planes_per_panel, cutoff, device);
+        *out = new psp_cu_handle{s};
+    });
+}
+
+void psp_cu_destroy(psp_cu_handle* h) {
+    if (!h) return;
+    delete h->solver;
+    delete h;
+}
+
+int psp_cu_initialize(psp_cu_handle* h, const double* velocity, int panel_scheme, int precision) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->Initialize(velocity, false, panel_scheme, precision); });
+}
+
+int psp_cu_initialize_device(psp_cu_handle* h, const double* d_velocity, int panel_scheme, int precision) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->Initialize(d_velocity, true, panel_scheme, precision); });
+}
+
+int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_cu_stats* stats) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!h->solver->Initialized()) throw PspError(PSP_CU_NOT_INITIALIZED, "DistHelmholtz is not initialized");
+        psp_b200::SolveStats s;
+        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->SolveDevice(d, k, m, rel_tol, &s); });
+        FillStats(s, stats);
+    });
+}
+
+int psp_cu_solve_device(psp_cu_handle* h, double* d_B, int k, int m, double rel_tol, psp_cu_stats* stats) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!d_B) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
+        psp_b200::SolveStats s;
+        h->solver->SolveDevice(reinterpret_cast<psp_b200::z64*>(d_B), k, m, rel_tol, &s);
+        FillStats(s, stats);
+    });
+}
+
+int psp_cu_finalize(psp_cu_handle* h) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->Finalize(); });
+}
+
+int psp_cu_multiply(psp_cu_handle* h, double* B, int k) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->MultiplyDevice(d, k); });
+    });
+}
+
+int psp_cu_precondition(psp_cu_handle* h, double* B, int k) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!h->solver->Initialized()) throw PspError(PSP_CU_NOT_INITIALIZED, "DistHelmholtz is not initialized");
+        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->PreconditionDevice(d, k); });
+    });
+}
+
+int psp_cu_multiply_device(psp_cu_handle* h, double* d_B, int k) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->MultiplyDevice(reinterpret_cast<psp_b200::z64*>(d_B), k); });
+}
+
+int psp_cu_precondition_device(psp_cu_handle* h, double* d_B, int k) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->PreconditionDevice(reinterpret_cast<psp_b200::z64*>(d_B), k); });
+}
+
+int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!h->solver->Initialized()) throw PspError(PSP_CU_NOT_INITIALIZED, "DistHelmholtz is not initialized");
+        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->SolvePanelDevice(d, k, panel); });
+    });
+}
+
+int psp_cu_set_max_iterations(psp_cu_handle* h, int max_iterations) {
+    if (int e = CheckHandle(h)) return e;
+    h->solver->SetMaxIterations(max_iterations);
+    return PSP_CU_OK;
+}
+
+int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info) {
+    if (int e = CheckHandle(h)) return e;
+    const psp_b200::PanelGeometry& g = h->solver->analysis().geom;
+    if (num_panels) *num_panels = g.numPanels;
+    if (info)
+        for (int p = 0; p < g.numPanels; ++p) {
+            info[4 * p + 0] = g.LowV(p);
+            info[4 * p + 1] = g.Depth(p);
+            info[4 * p + 2] = g.Padding(p);
+            info[4 * p + 3] = g.Class(p);
+        }
+    return PSP_CU_OK;
+}
+
+int psp_cu_analyze_class(const psp_cu_disc* disc, int planes_per_panel, int cutoff, int cls, int* num_nodes,
+                         int* vsize, int* info, int* nd_to_nat) {
+    if (!disc) {
+        g_lastError = "null argument";
+        return PSP_CU_LOGIC_ERROR;
+    }
+    return Guard([&] {
+        psp_b200::DiscParams d;
+        std::memcpy(&d, disc, sizeof(d));
+        psp_b200::Analysis an;
+        an.Build(d, planes_per_panel, cutoff);
+        if (cls < 0 || cls > 2 || !an.classUsed[cls]) throw std::logic_error("panel class not present");
+        const psp_b200::ClassStructure& cs = an.cls[cls];
+        const int nn = (int)an.tree.nodes.size();
+        if (num_nodes) *num_nodes = nn;
+        if (vsize) *vsize = cs.vSize;
+        if (info)
+            for (int t = 0; t < nn; ++t) {
+                info[4 * t + 0] = cs.off[t];
+                info[4 * t + 1] = cs.size[t];
+                info[4 * t + 2] = cs.usize[t];
+                info[4 * t + 3] = an.tree.nodes[t].parent;
+            }
+        if (nd_to_nat) std::memcpy(nd_to_nat, cs.ndToNat.data(), sizeof(int) * cs.ndToNat.size());
+    });
+}
+
+int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* factor_bytes) {
+    if (int e = CheckHandle(h)) return e;
+    if (setup_seconds) *setup_seconds = h->solver->setupSeconds();
+    if (factor_bytes) *factor_bytes = (long long)h->solver->factorBytes();
+    return PSP_CU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,162 @@
+// Device kernels of the sweeping-preconditioned Helmholtz solve and the
+// descriptors the host orchestration fills for them.  Every batched kernel
+// walks a task list, so one launch covers all fronts of one elimination-tree
+// depth across every panel (and every problem) in flight.
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+
+namespace psp_b200 {
+
+// ------------------------------------------------------------------ stencil
+
+// 1-D PML tables live on the device with one guard entry on each side:
+// table[i+1] holds the value at grid index i, i in [-1, n].
+struct StencilParams {
+    int nx, ny, nz;
+    double ihx2, ihy2, ihz2;  // 1/(2 h^2) per axis
+    double omega;
+    const z64* s1; const z64* is1;  // s1Inv and its reciprocal (initialize_finalize.hpp:415-441)
+    const z64* s2; const z64* is2;  // s2Inv (443-469)
+    const z64* s3; const z64* is3;  // s3Inv on the global sweep coordinate v (471-497)
+};
+
+// y := A x, or y := b - A x when b != nullptr, for natural-order grids with
+// k interleaved right-hand sides (Multiply, solve.hpp:613-679; the operator is
+// FormGlobalRow, initialize_finalize.hpp:527-587, evaluated on the fly).
+void LaunchHelmholtzApply(const z64* x, z64* y, const z64* b, const double* vel, const StencilParams& sp, int k,
+                          cudaStream_t st);
+
+// ------------------------------------------------------------------ batched GEMM
+
+// C = alpha * op(A) * diag(d) * op(B) + beta * C, complex, no conjugation.
+// lowerC restricts the update to row >= col.  triA/triB describe structural
+// zeros: triA 1 -> op(A)[r][k] = 0 for k > r, 2 -> for k < r;
+// triB 1 -> op(B)[k][c] = 0 for k < c, 2 -> for k > c.
+template <typename R>
+struct GemmOp {
+    const cpx<R>* A;
+    const cpx<R>* B;
+    cpx<R>* C;
+    const cpx<R>* d;
+    int64_t lda, ldb, ldc;
+    int M, N, K;
+    int transA, transB, lowerC, triA, triB;
+    R alpha_re, alpha_im, beta_re, beta_im;
+};
+struct GemmTile {
+    int op, tm, tn;
+};
+
+enum GemmShape { kGemmSquare = 0, kGemmSkinny = 1 };
+int GemmTileM(GemmShape s);
+int GemmTileN(GemmShape s);
+// Appends the output tiles of `op` (index opIndex) to `tiles`.
+template <typename R>
+void AppendGemmTiles(const GemmOp<R>& op, int opIndex, GemmShape shape, std::vector<GemmTile>& tiles);
+template <typename R>
+void LaunchGemm(const GemmOp<R>* ops, const GemmTile* tiles, int numTiles, GemmShape shape, cudaStream_t st);
+
+// ------------------------------------------------------------------ factorization
+
+constexpr int kNB = 32;  // column block of the frontal LDL^T
+
+// One front of one panel during the factorization (cliq::LDL replacement).
+template <typename R>
+struct FactorFront {
+    cpx<R>* L;      // transient (s+u) x s frontal columns, ld = s+u
+    cpx<R>* G;      // persistent (s+u) x s: [inv(L11); -L21 inv(L11)], ld = s+u
+    cpx<R>* D;      // persistent pivots, s entries
+    cpx<R>* U;      // u x u Schur complement (update matrix), ld = u
+    cpx<R>* T;      // inversion scratch
+    const int* rel; // u entries: row of each structure index in the parent front
+    int s, u;
+    int parent;     // index of the parent in the same descriptor array (-1 for a root)
+    int cls;        // panel class (tables below)
+    int ndOff;      // first ND index of the node in its class ordering
+    int vOffset;    // global sweep coordinate of the padded subproblem's first plane
+    int s3aOff;     // offset of the panel's artificial-PML table
+};
+
+struct ClassTables {
+    const int* ndToNat[3];
+    const int* nbrRows[3];
+};
+
+struct AssemblyParams {
+    StencilParams sp;
+    const double* vel;    // natural-order velocity
+    const z64* s3a;       // artificial s3Inv per panel, vSize+2 entries each
+    const z64* is3a;
+    double damping;
+    ClassTables tabs;
+};
+
+template <typename R>
+void LaunchAssemble(const FactorFront<R>* fronts, const int* list, int n, const AssemblyParams& ap,
+                    cudaStream_t st);
+// tasks: (child front, first update column)
+template <typename R>
+void LaunchExtendAdd(const FactorFront<R>* fronts, const int2* tasks, int n, cudaStream_t st);
+template <typename R>
+void LaunchLdlDiag(const FactorFront<R>* fronts, const int* list, int n, int J, int* status, cudaStream_t st);
+// tasks: (front, first row of a kTrsmRows-row tile below the diagonal block)
+constexpr int kTrsmRows = 32;
+template <typename R>
+void LaunchLdlTrsm(const FactorFront<R>* fronts, const int2* tasks, int n, int J, cudaStream_t st);
+
+// ------------------------------------------------------------------ panel solves
+
+// One front of the panel being solved (cliq::Solve replacement).
+template <typename R>
+struct SolveFront {
+    const cpx<R>* G;
+    const cpx<R>* D;
+    cpx<R>* Rv;      // (s+u) x k work vector, ld = s+u
+    cpx<R>* Ov;      // (s+u) x k work vector, ld = s+u
+    const int* rel;
+    int s, u, ndOff, parent, child0, child1;
+};
+
+struct PanelIO {
+    const int* ndToNat;
+    int nxy, nx, nz;
+    int ldk;         // row stride (complex entries per point) of the natural-order grid
+    int padding;     // leading planes of the subproblem that are artificial padding
+    int vOffset;     // global v of the subproblem's first plane
+    int lowV, highV; // global v range of the panel's own planes
+    int inMode;      // 0: B_i; 1: B_i - A_{i,i-1} B_{i-1}; 2: -A_{i,i+1} B_{i+1} only
+    int outAccumulate;
+    StencilParams sp;
+};
+
+template <typename R>
+void LaunchForwardGather(const SolveFront<R>* fr, const int2* tasks, int n, const z64* B, int k, PanelIO io,
+                         cudaStream_t st);
+template <typename R>
+void LaunchBackwardGather(const SolveFront<R>* fr, const int2* tasks, int n, int k, cudaStream_t st);
+template <typename R>
+void LaunchScatter(const SolveFront<R>* fr, const int2* tasks, int n, z64* B, int k, PanelIO io, cudaStream_t st);
+constexpr int kSolveRowTile = 64;
+
+// ------------------------------------------------------------------ GMRES vectors
+
+// Per-RHS reductions over natural-order [N][k] vectors; partial sums per block
+// land in `partial` (gridDim x k) and a second pass sums them in fixed order.
+int ReduceBlocks(int64_t npoints, int k);
+void LaunchNormsPartial(const z64* w, int64_t npoints, int k, double* partial, cudaStream_t st);
+void LaunchSumPartialReal(const double* partial, int nblocks, int k, double* out, int sqrtOut, cudaStream_t st);
+// w -= h_prev (.) v_prev (if v_prev) and partial dots conj(v_next) . w
+void LaunchMgsStep(z64* w, const z64* v_prev, const z64* h_prev, const z64* v_next, int64_t npoints, int k,
+                   z64* partial, cudaStream_t st);
+void LaunchSumPartialComplex(const z64* partial, int nblocks, int k, z64* out, cudaStream_t st);
+// v := w / s (per RHS, s real)
+void LaunchScaleColumns(const z64* w, const double* s, z64* v, int64_t npoints, int k, cudaStream_t st);
+// x := x0 + sum_i y[i,r] V_i[:,r]
+void LaunchCombine(const z64* x0, const z64* V, int64_t vstride, const z64* y, int j1, z64* x, int64_t npoints,
+                   int k, cudaStream_t st);
+// w := w - h (.) v   (final MGS axpy)
+void LaunchAxpyColumns(z64* w, const z64* v, const z64* h, int64_t npoints, int k, cudaStream_t st);
+
+}  // namespace psp_b200

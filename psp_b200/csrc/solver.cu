@@ -1,0 +1,911 @@
+// Host orchestration of the B200 sweeping-preconditioned Helmholtz solve:
+// table upload, depth-batched multifrontal factorization of every panel,
+// the sweep (Precondition, solve.hpp:681-734) and multi-RHS GMRES(m)
+// (InternalSolveWithGMRES, solve.hpp:241-611).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "solver.hpp"
+
+namespace psp_b200 {
+
+void DeviceBuffer::Allocate(size_t n) {
+    Release();
+    if (n == 0) n = 256;
+    CUDA_CHECK(cudaMalloc(&p, n));
+    bytes = n;
+}
+
+void DeviceBuffer::Release() {
+    if (p) {
+        cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+}
+
+void TaskArena::Upload(cudaStream_t st) {
+    if (host.empty()) host.resize(256);
+    if (dev.bytes < host.size()) dev.Allocate(host.size());
+    CUDA_CHECK(cudaMemcpyAsync(dev.p, host.data(), host.size(), cudaMemcpyHostToDevice, st));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+namespace {
+
+typedef std::complex<double> Cd;
+
+// Imaginary stretch of a PML point at distance `delta` from the inner edge
+// (the common body of s1Inv/s2Inv/s3Inv/s3InvArtificial,
+// initialize_finalize.hpp:415-525).
+Cd PmlPoint(double delta, int b, double sigma, double h, double omega) {
+    const double eta = b * h;
+    return Cd(1.0, (sigma / eta) * (delta / b) * (delta / b) * (2 * M_PI / omega));
+}
+
+// Value of a 1-D stretch at grid index i (low face active for i < b-1 + lowShift).
+Cd Stretch(int i, int n, int b, double sigma, double h, double omega, bool lowPML, bool highPML, int lowEdge) {
+    if (lowPML && i < lowEdge + b - 1) return PmlPoint((lowEdge + b - 1) - i, b, sigma, h, omega);
+    if (highPML && i > n - b) return PmlPoint(i - (n - b), b, sigma, h, omega);
+    return Cd(1.0, 0.0);
+}
+
+void PushTable(std::vector<z64>& vals, std::vector<z64>& invs, const std::vector<Cd>& t) {
+    for (const Cd& c : t) {
+        vals.push_back(mk(c.real(), c.imag()));
+        const Cd inv = 1.0 / c;
+        invs.push_back(mk(inv.real(), inv.imag()));
+    }
+}
+
+template <typename T>
+void UploadVector(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t st) {
+    buf.Allocate(std::max<size_t>(v.size() * sizeof(T), 256));
+    if (!v.empty()) CUDA_CHECK(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+template <typename R>
+GemmOp<R> MakeOp(const cpx<R>* A, int64_t lda, int transA, const cpx<R>* B, int64_t ldb, int transB, cpx<R>* C,
+                 int64_t ldc, int M, int N, int K, R alpha, R beta) {
+    GemmOp<R> op;
+    std::memset(&op, 0, sizeof(op));
+    op.A = A; op.lda = lda; op.transA = transA;
+    op.B = B; op.ldb = ldb; op.transB = transB;
+    op.C = C; op.ldc = ldc;
+    op.M = M; op.N = N; op.K = K;
+    op.alpha_re = alpha; op.beta_re = beta;
+    return op;
+}
+
+}  // namespace
+
+// =====================================================================
+// Factor store: persistent G (selectively inverted factors) and D per
+// panel, the factorization schedule and the panel solves.
+// =====================================================================
+
+template <typename R>
+class FactorStore {
+public:
+    explicit FactorStore(Helmholtz& h) : h_(h), an_(h.an_) {}
+    void Factor();
+    void SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc);
+    void Sweep(z64* B, int ldk, int k);
+    int64_t Bytes() const { return (int64_t)(G_.bytes + D_.bytes); }
+
+private:
+    struct Step {
+        enum Kind { kMemset, kAssemble, kExtend, kDiag, kTrsm, kGemm } kind;
+        size_t a = 0, b = 0;
+        int n = 0, J = 0;
+        size_t bytes = 0;
+    };
+    void FactorGroup(int p0, int p1, FactorFront<R>* hostFronts, std::vector<FactorFront<R>>& all);
+    void BuildSolvePlan(int k);
+
+    Helmholtz& h_;
+    const Analysis& an_;
+    int nn_ = 0;  // nodes per panel tree
+    DeviceBuffer G_, D_;
+    std::vector<int64_t> gOff_, dOff_;
+    std::vector<std::vector<int>> depthNodes_;
+    DeviceBuffer status_;
+    // solve plan for one RHS block width
+    int planK_ = -1;
+    DeviceBuffer Rv_, Ov_;
+    TaskArena solveArena_;
+    struct ClassPlan {
+        std::vector<size_t> fg, fTiles, bTiles;
+        std::vector<int> fgN, fTilesN, bTilesN;
+        size_t sc = 0;
+        int scN = 0;
+    } cplan_[3];
+    std::vector<size_t> panelFronts_, panelFwdOps_, panelBwdOps_;
+};
+
+template <typename R>
+void FactorStore<R>::Factor() {
+    const PanelGeometry& g = an_.geom;
+    const XYTree& tree = an_.tree;
+    nn_ = (int)tree.nodes.size();
+    const int np = g.numPanels;
+    depthNodes_.assign(tree.maxDepth + 1, {});
+    for (int t = 0; t < nn_; ++t) depthNodes_[tree.nodes[t].depth].push_back(t);
+
+    gOff_.assign((size_t)np * nn_, 0);
+    dOff_.assign((size_t)np * nn_, 0);
+    int64_t gTot = 0, dTot = 0;
+    for (int p = 0; p < np; ++p) {
+        const ClassStructure& cs = an_.cls[g.Class(p)];
+        for (int t = 0; t < nn_; ++t) {
+            gOff_[(size_t)p * nn_ + t] = gTot;
+            dOff_[(size_t)p * nn_ + t] = dTot;
+            gTot += (int64_t)(cs.size[t] + cs.usize[t]) * cs.size[t];
+            dTot += cs.size[t];
+        }
+    }
+    G_.Allocate(gTot * sizeof(cpx<R>));
+    D_.Allocate(dTot * sizeof(cpx<R>));
+    CUDA_CHECK(cudaMemsetAsync(G_.p, 0, G_.bytes, h_.stream_));
+    status_.Allocate(sizeof(int));
+    CUDA_CHECK(cudaMemsetAsync(status_.p, 0, sizeof(int), h_.stream_));
+
+    std::vector<FactorFront<R>> all((size_t)np * nn_);
+    for (int p = 0; p < np; ++p) {
+        const int c = g.Class(p);
+        const ClassStructure& cs = an_.cls[c];
+        for (int t = 0; t < nn_; ++t) {
+            FactorFront<R>& f = all[(size_t)p * nn_ + t];
+            std::memset(&f, 0, sizeof(f));
+            f.G = G_.as<cpx<R>>() + gOff_[(size_t)p * nn_ + t];
+            f.D = D_.as<cpx<R>>() + dOff_[(size_t)p * nn_ + t];
+            f.rel = h_.dRel_[c].as<int>() + cs.lowerOff[t];
+            f.s = cs.size[t];
+            f.u = cs.usize[t];
+            f.parent = tree.nodes[t].parent < 0 ? -1 : p * nn_ + tree.nodes[t].parent;
+            f.cls = c;
+            f.ndOff = cs.off[t];
+            f.vOffset = g.SubVOffset(p);
+            f.s3aOff = h_.s3aOff_[p];
+        }
+    }
+    // Transient bytes a group of panels needs at its busiest depth.
+    auto transient = [&](int p0, int p1) {
+        std::vector<int64_t> L(depthNodes_.size(), 0), U(depthNodes_.size(), 0), T(depthNodes_.size(), 0);
+        for (size_t d = 0; d < depthNodes_.size(); ++d)
+            for (int p = p0; p < p1; ++p) {
+                const ClassStructure& cs = an_.cls[g.Class(p)];
+                for (int t : depthNodes_[d]) {
+                    const int64_t s = cs.size[t], u = cs.usize[t];
+                    L[d] += (s + u) * s;
+                    U[d] += u * u;
+                    T[d] += (s / 2 + 1) * (s / 2 + 1) * 2;
+                }
+            }
+        int64_t ua = 0, ub = 0, lm = 0, tm = 0;
+        for (size_t d = 0; d < depthNodes_.size(); ++d) {
+            (d % 2 ? ub : ua) = std::max(d % 2 ? ub : ua, U[d]);
+            lm = std::max(lm, L[d]);
+            tm = std::max(tm, T[d]);
+        }
+        return (ua + ub + lm + tm) * (int64_t)sizeof(cpx<R>);
+    };
+    size_t freeB = 0, totalB = 0;
+    CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
+    const int64_t budget = (int64_t)(freeB * 0.8);
+    int groupSize = np;
+    while (groupSize > 1 && transient(0, groupSize) > budget) groupSize = (groupSize + 1) / 2;
+    for (int p0 = 0; p0 < np; p0 += groupSize) FactorGroup(p0, std::min(np, p0 + groupSize), nullptr, all);
+    int st = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, h_.stream_));
+    CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
+    if (st) throw PspError(kRuntimeError, "zero or non-finite pivot in a panel factorization");
+}
+
+template <typename R>
+void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<FactorFront<R>>& all) {
+    const PanelGeometry& g = an_.geom;
+    const XYTree& tree = an_.tree;
+    const int nd = (int)depthNodes_.size();
+    cudaStream_t st = h_.stream_;
+    // per-depth transient layout
+    std::vector<int64_t> Lsz(nd, 0), Usz(nd, 0), Tsz(nd, 0);
+    std::vector<int64_t> Lpos((size_t)(p1 - p0) * nn_), Upos((size_t)(p1 - p0) * nn_), Tpos((size_t)(p1 - p0) * nn_);
+    for (int d = 0; d < nd; ++d)
+        for (int p = p0; p < p1; ++p) {
+            const ClassStructure& cs = an_.cls[g.Class(p)];
+            for (int t : depthNodes_[d]) {
+                const int64_t s = cs.size[t], u = cs.usize[t];
+                const size_t i = (size_t)(p - p0) * nn_ + t;
+                Lpos[i] = Lsz[d]; Lsz[d] += (s + u) * s;
+                Upos[i] = Usz[d]; Usz[d] += u * u;
+                Tpos[i] = Tsz[d]; Tsz[d] += (s / 2 + 1) * (s / 2 + 1) * 2;
+            }
+        }
+    int64_t ua = 0, ub = 0, lm = 0, tm = 0;
+    for (int d = 0; d < nd; ++d) {
+        if (d % 2) ub = std::max(ub, Usz[d]); else ua = std::max(ua, Usz[d]);
+        lm = std::max(lm, Lsz[d]);
+        tm = std::max(tm, Tsz[d]);
+    }
+    DeviceBuffer arena;
+    arena.Allocate((ua + ub + lm + tm) * sizeof(cpx<R>));
+    cpx<R>* UA = arena.as<cpx<R>>();
+    cpx<R>* UB = UA + ua;
+    cpx<R>* Lb = UB + ub;
+    cpx<R>* Tb = Lb + lm;
+    for (int d = 0; d < nd; ++d)
+        for (int p = p0; p < p1; ++p)
+            for (int t : depthNodes_[d]) {
+                const size_t i = (size_t)(p - p0) * nn_ + t;
+                FactorFront<R>& f = all[(size_t)p * nn_ + t];
+                f.L = Lb + Lpos[i];
+                f.U = (d % 2 ? UB : UA) + Upos[i];
+                f.T = Tb + Tpos[i];
+            }
+
+    TaskArena arenaTasks;
+    const size_t frontsOff = arenaTasks.Push(all);
+    std::vector<Step> steps;
+    std::vector<GemmOp<R>> ops;
+    std::vector<GemmTile> tiles;
+    auto pushGemm = [&]() {
+        if (tiles.empty()) { ops.clear(); return; }
+        Step s;
+        s.kind = Step::kGemm;
+        s.a = arenaTasks.Push(ops);
+        s.b = arenaTasks.Push(tiles);
+        s.n = (int)tiles.size();
+        steps.push_back(s);
+        ops.clear();
+        tiles.clear();
+    };
+    auto addOp = [&](const GemmOp<R>& op) {
+        AppendGemmTiles(op, (int)ops.size(), kGemmSquare, tiles);
+        ops.push_back(op);
+    };
+    const R one = 1, mone = -1, zero = 0;
+    for (int d = nd - 1; d >= 0; --d) {
+        std::vector<int> list;
+        int maxS = 0;
+        for (int p = p0; p < p1; ++p)
+            for (int t : depthNodes_[d]) {
+                list.push_back(p * nn_ + t);
+                maxS = std::max(maxS, all[(size_t)p * nn_ + t].s);
+            }
+        if (list.empty()) continue;
+        // zero this depth's frontal columns and update matrices
+        {
+            Step s;
+            s.kind = Step::kMemset;
+            s.a = (size_t)((char*)Lb - (char*)arena.p);
+            s.bytes = Lsz[d] * sizeof(cpx<R>);
+            steps.push_back(s);
+            s.a = (size_t)((char*)(d % 2 ? UB : UA) - (char*)arena.p);
+            s.bytes = Usz[d] * sizeof(cpx<R>);
+            steps.push_back(s);
+        }
+        {
+            Step s;
+            s.kind = Step::kAssemble;
+            s.a = arenaTasks.Push(list);
+            s.n = (int)list.size();
+            steps.push_back(s);
+        }
+        for (int slot = 0; slot < 2; ++slot) {
+            std::vector<int2> ext;
+            for (int fi : list) {
+                const int t = fi % nn_, p = fi / nn_;
+                const XYNode& node = tree.nodes[t];
+                if (node.numChildren <= slot) continue;
+                const int ci = p * nn_ + node.child[slot];
+                for (int b0 = 0; b0 < all[ci].u; b0 += 32) ext.push_back(make_int2(ci, b0));
+            }
+            if (ext.empty()) continue;
+            Step s;
+            s.kind = Step::kExtend;
+            s.a = arenaTasks.Push(ext);
+            s.n = (int)ext.size();
+            steps.push_back(s);
+        }
+        // right-looking blocked LDL^T over the pivot columns
+        for (int J = 0; J < maxS; J += kNB) {
+            std::vector<int> dl;
+            std::vector<int2> tr;
+            for (int fi : list) {
+                const FactorFront<R>& f = all[fi];
+                if (f.s <= J) continue;
+                dl.push_back(fi);
+                const int b = std::min(kNB, f.s - J);
+                for (int r0 = J + b; r0 < f.s + f.u; r0 += kTrsmRows) tr.push_back(make_int2(fi, r0));
+                const int M = f.s + f.u - J - b, N = f.s - J - b;
+                if (M > 0 && N > 0) {
+                    const int64_t ld = f.s + f.u;
+                    GemmOp<R> op = MakeOp<R>(f.L + (J + b) + J * ld, ld, 0, f.L + (J + b) + J * ld, ld, 1,
+                                             f.L + (J + b) + (J + b) * ld, ld, M, N, b, mone, one);
+                    op.d = f.D + J;
+                    op.lowerC = 1;
+                    addOp(op);
+                }
+            }
+            Step s;
+            s.kind = Step::kDiag;
+            s.a = arenaTasks.Push(dl);
+            s.n = (int)dl.size();
+            s.J = J;
+            steps.push_back(s);
+            if (!tr.empty()) {
+                Step t;
+                t.kind = Step::kTrsm;
+                t.a = arenaTasks.Push(tr);
+                t.n = (int)tr.size();
+                t.J = J;
+                steps.push_back(t);
+            }
+            pushGemm();
+        }
+        // inv(L11) by recursive doubling of the kNB diagonal inverses
+        for (int S = kNB; S < maxS; S *= 2) {
+            std::vector<GemmOp<R>> ops2;
+            std::vector<GemmTile> tiles2;
+            for (int fi : list) {
+                const FactorFront<R>& f = all[fi];
+                const int64_t ld = f.s + f.u;
+                int64_t toff = 0;
+                for (int a0 = 0; a0 + S < f.s; a0 += 2 * S) {
+                    const int a1 = a0 + S, a2 = std::min(a0 + 2 * S, f.s);
+                    const int m = a2 - a1, n = a1 - a0;
+                    cpx<R>* T = f.T + toff;
+                    toff += (int64_t)m * n;
+                    GemmOp<R> op1 = MakeOp<R>(f.L + a1 + a0 * ld, ld, 0, f.G + a0 + a0 * ld, ld, 0, T, m, m, n, n,
+                                              one, zero);
+                    op1.triB = 1;
+                    addOp(op1);
+                    GemmOp<R> op2 = MakeOp<R>(f.G + a1 + a1 * ld, ld, 0, T, m, 0, f.G + a1 + a0 * ld, ld, m, n, m,
+                                              mone, zero);
+                    op2.triA = 1;
+                    AppendGemmTiles(op2, (int)ops2.size(), kGemmSquare, tiles2);
+                    ops2.push_back(op2);
+                }
+            }
+            pushGemm();
+            ops = ops2;
+            tiles = tiles2;
+            pushGemm();
+        }
+        // G21 = -L21 inv(L11) and the Schur complement U -= L21 D L21^T
+        for (int fi : list) {
+            const FactorFront<R>& f = all[fi];
+            if (f.u == 0) continue;
+            const int64_t ld = f.s + f.u;
+            GemmOp<R> g21 = MakeOp<R>(f.L + f.s, ld, 0, f.G, ld, 0, f.G + f.s, ld, f.u, f.s, f.s, mone, zero);
+            g21.triB = 1;
+            addOp(g21);
+            GemmOp<R> sch = MakeOp<R>(f.L + f.s, ld, 0, f.L + f.s, ld, 1, f.U, f.u, f.u, f.u, f.s, mone, one);
+            sch.d = f.D;
+            sch.lowerC = 1;
+            addOp(sch);
+        }
+        pushGemm();
+    }
+    arenaTasks.Upload(st);
+    const FactorFront<R>* dFronts = arenaTasks.At<FactorFront<R>>(frontsOff);
+    for (const Step& s : steps) {
+        switch (s.kind) {
+            case Step::kMemset:
+                if (s.bytes) CUDA_CHECK(cudaMemsetAsync((char*)arena.p + s.a, 0, s.bytes, st));
+                break;
+            case Step::kAssemble:
+                LaunchAssemble<R>(dFronts, arenaTasks.At<int>(s.a), s.n, h_.ap_, st);
+                break;
+            case Step::kExtend:
+                LaunchExtendAdd<R>(dFronts, arenaTasks.At<int2>(s.a), s.n, st);
+                break;
+            case Step::kDiag:
+                LaunchLdlDiag<R>(dFronts, arenaTasks.At<int>(s.a), s.n, s.J, status_.as<int>(), st);
+                break;
+            case Step::kTrsm:
+                LaunchLdlTrsm<R>(dFronts, arenaTasks.At<int2>(s.a), s.n, s.J, st);
+                break;
+            case Step::kGemm:
+                LaunchGemm<R>(arenaTasks.At<GemmOp<R>>(s.a), arenaTasks.At<GemmTile>(s.b), s.n, kGemmSquare, st);
+                break;
+        }
+    }
+    CUDA_CHECK(cudaStreamSynchronize(st));
+}
+
+template <typename R>
+void FactorStore<R>::BuildSolvePlan(int k) {
+    if (planK_ == k) return;
+    const PanelGeometry& g = an_.geom;
+    const XYTree& tree = an_.tree;
+    const int np = g.numPanels;
+    const int nd = (int)depthNodes_.size();
+    std::vector<std::vector<int64_t>> vecOff(3);
+    int64_t maxVec = 0;
+    for (int c = 0; c < 3; ++c) {
+        if (!an_.classUsed[c]) continue;
+        const ClassStructure& cs = an_.cls[c];
+        vecOff[c].resize(nn_);
+        int64_t tot = 0;
+        for (int t = 0; t < nn_; ++t) {
+            vecOff[c][t] = tot;
+            tot += (int64_t)(cs.size[t] + cs.usize[t]) * k;
+        }
+        maxVec = std::max(maxVec, tot);
+    }
+    Rv_.Allocate(maxVec * sizeof(cpx<R>));
+    Ov_.Allocate(maxVec * sizeof(cpx<R>));
+    solveArena_.host.clear();
+    panelFronts_.assign(np, 0);
+    panelFwdOps_.assign(np, 0);
+    panelBwdOps_.assign(np, 0);
+    for (int p = 0; p < np; ++p) {
+        const int c = g.Class(p);
+        const ClassStructure& cs = an_.cls[c];
+        std::vector<SolveFront<R>> fr(nn_);
+        std::vector<GemmOp<R>> fo(nn_), bo(nn_);
+        for (int t = 0; t < nn_; ++t) {
+            SolveFront<R>& f = fr[t];
+            const XYNode& node = tree.nodes[t];
+            f.G = G_.as<cpx<R>>() + gOff_[(size_t)p * nn_ + t];
+            f.D = D_.as<cpx<R>>() + dOff_[(size_t)p * nn_ + t];
+            f.Rv = Rv_.as<cpx<R>>() + vecOff[c][t];
+            f.Ov = Ov_.as<cpx<R>>() + vecOff[c][t];
+            f.rel = h_.dRel_[c].as<int>() + cs.lowerOff[t];
+            f.s = cs.size[t];
+            f.u = cs.usize[t];
+            f.ndOff = cs.off[t];
+            f.parent = node.parent;
+            f.child0 = node.numChildren > 0 ? node.child[0] : -1;
+            f.child1 = node.numChildren > 1 ? node.child[1] : -1;
+            const int64_t ld = f.s + f.u;
+            fo[t] = MakeOp<R>(f.G, ld, 0, f.Rv, ld, 0, f.Ov, ld, f.s + f.u, k, f.s, R(1), R(1));
+            fo[t].triA = 1;
+            bo[t] = MakeOp<R>(f.G, ld, 1, f.Ov, ld, 0, f.Rv, ld, f.s, k, f.s + f.u, R(1), R(0));
+            bo[t].triA = 2;
+        }
+        panelFronts_[p] = solveArena_.Push(fr);
+        panelFwdOps_[p] = solveArena_.Push(fo);
+        panelBwdOps_[p] = solveArena_.Push(bo);
+    }
+    for (int c = 0; c < 3; ++c) {
+        if (!an_.classUsed[c]) continue;
+        const ClassStructure& cs = an_.cls[c];
+        ClassPlan& cp = cplan_[c];
+        cp.fg.assign(nd, 0); cp.fTiles.assign(nd, 0); cp.bTiles.assign(nd, 0);
+        cp.fgN.assign(nd, 0); cp.fTilesN.assign(nd, 0); cp.bTilesN.assign(nd, 0);
+        for (int d = 0; d < nd; ++d) {
+            std::vector<int2> gt;
+            std::vector<GemmTile> ft, bt;
+            for (int t : depthNodes_[d]) {
+                const int s = cs.size[t], u = cs.usize[t];
+                for (int i0 = 0; i0 < s + u; i0 += kSolveRowTile) gt.push_back(make_int2(t, i0));
+                GemmOp<R> fo = MakeOp<R>(nullptr, 1, 0, nullptr, 1, 0, nullptr, 1, s + u, k, s, R(1), R(1));
+                GemmOp<R> bo = MakeOp<R>(nullptr, 1, 1, nullptr, 1, 0, nullptr, 1, s, k, s + u, R(1), R(0));
+                AppendGemmTiles(fo, t, kGemmSkinny, ft);
+                AppendGemmTiles(bo, t, kGemmSkinny, bt);
+            }
+            cp.fg[d] = solveArena_.Push(gt);
+            cp.fgN[d] = (int)gt.size();
+            cp.fTiles[d] = solveArena_.Push(ft);
+            cp.fTilesN[d] = (int)ft.size();
+            cp.bTiles[d] = solveArena_.Push(bt);
+            cp.bTilesN[d] = (int)bt.size();
+        }
+        std::vector<int2> sc;
+        for (int t = 0; t < nn_; ++t)
+            for (int i0 = 0; i0 < cs.size[t]; i0 += kSolveRowTile) sc.push_back(make_int2(t, i0));
+        cp.sc = solveArena_.Push(sc);
+        cp.scN = (int)sc.size();
+    }
+    solveArena_.Upload(h_.stream_);
+    planK_ = k;
+}
+
+template <typename R>
+void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc) {
+    BuildSolvePlan(k);
+    const PanelGeometry& g = an_.geom;
+    const int c = g.Class(p);
+    const ClassPlan& cp = cplan_[c];
+    cudaStream_t st = h_.stream_;
+    PanelIO io;
+    io.ndToNat = h_.dNdToNat_[c].as<int>();
+    io.nx = an_.disc.nx;
+    io.nxy = an_.disc.nx * an_.disc.ny;
+    io.nz = an_.disc.nz;
+    io.ldk = ldk;
+    io.padding = g.Padding(p);
+    io.vOffset = g.SubVOffset(p);
+    io.lowV = g.LowV(p);
+    io.highV = g.LowV(p) + g.Depth(p) - 1;
+    io.inMode = inMode;
+    io.outAccumulate = outAcc;
+    io.sp = h_.sp_;
+    const SolveFront<R>* fr = solveArena_.At<SolveFront<R>>(panelFronts_[p]);
+    const GemmOp<R>* fo = solveArena_.At<GemmOp<R>>(panelFwdOps_[p]);
+    const GemmOp<R>* bo = solveArena_.At<GemmOp<R>>(panelBwdOps_[p]);
+    const int nd = (int)depthNodes_.size();
+    for (int d = nd - 1; d >= 0; --d) {
+        LaunchForwardGather<R>(fr, solveArena_.At<int2>(cp.fg[d]), cp.fgN[d], B, k, io, st);
+        LaunchGemm<R>(fo, solveArena_.At<GemmTile>(cp.fTiles[d]), cp.fTilesN[d], kGemmSkinny, st);
+    }
+    for (int d = 0; d < nd; ++d) {
+        LaunchBackwardGather<R>(fr, solveArena_.At<int2>(cp.fg[d]), cp.fgN[d], k, st);
+        LaunchGemm<R>(bo, solveArena_.At<GemmTile>(cp.bTiles[d]), cp.bTilesN[d], kGemmSkinny, st);
+    }
+    LaunchScatter<R>(fr, solveArena_.At<int2>(cp.sc), cp.scN, B, k, io, st);
+}
+
+template <typename R>
+void FactorStore<R>::Sweep(z64* B, int ldk, int k) {
+    const int np = an_.geom.numPanels;
+    for (int i = 0; i < np - 1; ++i) SolvePanel(B, ldk, k, i, i == 0 ? 0 : 1, 0);
+    SolvePanel(B, ldk, k, np - 1, np - 1 == 0 ? 0 : 1, 0);
+    for (int i = np - 2; i >= 0; --i) SolvePanel(B, ldk, k, i, 2, 1);
+}
+
+template class FactorStore<double>;
+template class FactorStore<float>;
+
+// =====================================================================
+// Helmholtz
+// =====================================================================
+
+Helmholtz::Helmholtz(const DiscParams& d, double damping, int planesPerPanel, int cutoff, int device)
+    : damping_(damping), device_(device) {
+    an_.Build(d, planesPerPanel, cutoff);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw PspError(kNoDevice, "no CUDA device");
+    if (device < 0 || device >= count) throw PspError(kLogicError, "invalid CUDA device index");
+    CUDA_CHECK(cudaSetDevice(device));
+    CUDA_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    BuildTables();
+}
+
+Helmholtz::~Helmholtz() {
+    cudaSetDevice(device_);
+    f64_.reset();
+    f32_.reset();
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Helmholtz::BuildTables() {
+    const DiscParams& d = an_.disc;
+    const double hx = d.wx / (d.nx + 1), hy = d.wy / (d.ny + 1), hz = d.wz / (d.nz + 1);
+    std::vector<Cd> t1, t2, t3;
+    for (int i = -1; i <= d.nx; ++i)
+        t1.push_back(Stretch(i, d.nx, d.bx, d.sigmax, hx, d.omega, d.frontBC == kPML, d.backBC == kPML, 0));
+    for (int i = -1; i <= d.ny; ++i)
+        t2.push_back(Stretch(i, d.ny, d.by, d.sigmay, hy, d.omega, d.leftBC == kPML, d.rightBC == kPML, 0));
+    for (int i = -1; i <= d.nz; ++i)
+        t3.push_back(Stretch(i, d.nz, d.bz, d.sigmaz, hz, d.omega, true, d.topBC == kPML, 0));
+    std::vector<z64> v, iv;
+    PushTable(v, iv, t1);
+    v.insert(v.end(), iv.begin(), iv.end());
+    UploadVector(dS1_, v, stream_);
+    v.clear(); iv.clear();
+    PushTable(v, iv, t2);
+    v.insert(v.end(), iv.begin(), iv.end());
+    UploadVector(dS2_, v, stream_);
+    v.clear(); iv.clear();
+    PushTable(v, iv, t3);
+    v.insert(v.end(), iv.begin(), iv.end());
+    UploadVector(dS3_, v, stream_);
+    // artificial-PML tables of every panel subproblem (s3InvArtificial)
+    const PanelGeometry& g = an_.geom;
+    std::vector<Cd> ta;
+    s3aOff_.assign(g.numPanels, 0);
+    for (int p = 0; p < g.numPanels; ++p) {
+        s3aOff_[p] = (int)ta.size();
+        const int vSize = g.ClassVSize(g.Class(p)), vOff = g.SubVOffset(p);
+        for (int i = -1; i <= vSize; ++i)
+            ta.push_back(Stretch(vOff + i, d.nz, d.bz, d.sigmaz, hz, d.omega, true, d.topBC == kPML, vOff));
+    }
+    v.clear(); iv.clear();
+    PushTable(v, iv, ta);
+    const int na = (int)ta.size();
+    v.insert(v.end(), iv.begin(), iv.end());
+    UploadVector(dS3a_, v, stream_);
+
+    sp_.nx = d.nx; sp_.ny = d.ny; sp_.nz = d.nz;
+    sp_.ihx2 = 1.0 / (2 * hx * hx);
+    sp_.ihy2 = 1.0 / (2 * hy * hy);
+    sp_.ihz2 = 1.0 / (2 * hz * hz);
+    sp_.omega = d.omega;
+    sp_.s1 = dS1_.as<z64>(); sp_.is1 = sp_.s1 + (d.nx + 2);
+    sp_.s2 = dS2_.as<z64>(); sp_.is2 = sp_.s2 + (d.ny + 2);
+    sp_.s3 = dS3_.as<z64>(); sp_.is3 = sp_.s3 + (d.nz + 2);
+    for (int c = 0; c < 3; ++c) {
+        if (!an_.classUsed[c]) continue;
+        UploadVector(dNdToNat_[c], an_.cls[c].ndToNat, stream_);
+        UploadVector(dNbrRows_[c], an_.cls[c].nbrRows, stream_);
+        UploadVector(dRel_[c], an_.cls[c].rel, stream_);
+        ap_.tabs.ndToNat[c] = dNdToNat_[c].as<int>();
+        ap_.tabs.nbrRows[c] = dNbrRows_[c].as<int>();
+    }
+    ap_.sp = sp_;
+    ap_.s3a = dS3a_.as<z64>();
+    ap_.is3a = ap_.s3a + na;
+    ap_.damping = damping_;
+}
+
+void Helmholtz::Initialize(const double* velocity, bool devicePtr, int panelScheme, int precision) {
+    CUDA_CHECK(cudaSetDevice(device_));
+    const auto t0 = std::chrono::steady_clock::now();
+    if (an_.disc.omega == 0) throw PspError(kLogicError, "PML does not work at zero frequency");
+    if (panelScheme < 0 || panelScheme > 1) throw PspError(kLogicError, "Invalid panelScheme value");
+    if (precision < 0 || precision > 1) throw PspError(kLogicError, "Invalid precision mode");
+    if (!velocity) throw PspError(kLogicError, "Velocity grid is incorrect");
+    Finalize();
+    const int64_t N = NumUnknowns();
+    dVel_.Allocate(N * sizeof(double));
+    CUDA_CHECK(cudaMemcpyAsync(dVel_.p, velocity, N * sizeof(double),
+                               devicePtr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    ap_.vel = dVel_.as<double>();
+    precision_ = precision;
+    if (precision == 0) {
+        f64_.reset(new FactorStore<double>(*this));
+        f64_->Factor();
+    } else {
+        f32_.reset(new FactorStore<float>(*this));
+        f32_->Factor();
+    }
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+    initialized_ = true;
+    setupSeconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Helmholtz::Finalize() {
+    f64_.reset();
+    f32_.reset();
+    initialized_ = false;
+}
+
+int64_t Helmholtz::factorBytes() const {
+    if (f64_) return f64_->Bytes();
+    if (f32_) return f32_->Bytes();
+    return 0;
+}
+
+void Helmholtz::Precondition(z64* B, int k) {
+    constexpr int kBlock = 64;
+    for (int r0 = 0; r0 < k; r0 += kBlock) {
+        const int kb = std::min(kBlock, k - r0);
+        if (f64_) f64_->Sweep(B + r0, k, kb);
+        else f32_->Sweep(B + r0, k, kb);
+    }
+}
+
+void Helmholtz::PreconditionDevice(z64* B, int k) {
+    if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    CUDA_CHECK(cudaSetDevice(device_));
+    Precondition(B, k);
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+void Helmholtz::SolvePanelDevice(z64* B, int k, int panel) {
+    if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    if (panel < 0 || panel >= an_.geom.numPanels) throw PspError(kLogicError, "panel index out of range");
+    CUDA_CHECK(cudaSetDevice(device_));
+    constexpr int kBlock = 64;
+    for (int r0 = 0; r0 < k; r0 += kBlock) {
+        const int kb = std::min(kBlock, k - r0);
+        if (f64_) f64_->SolvePanel(B + r0, k, kb, panel, 0, 0);
+        else f32_->SolvePanel(B + r0, k, kb, panel, 0, 0);
+    }
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+void Helmholtz::MultiplyDevice(z64* B, int k) {
+    if (!dVel_.p) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    CUDA_CHECK(cudaSetDevice(device_));
+    const int64_t nk = NumUnknowns() * k;
+    DeviceBuffer tmp;
+    tmp.Allocate(nk * sizeof(z64));
+    LaunchHelmholtzApply(B, tmp.as<z64>(), nullptr, dVel_.as<double>(), sp_, k, stream_);
+    CUDA_CHECK(cudaMemcpyAsync(B, tmp.p, nk * sizeof(z64), cudaMemcpyDeviceToDevice, stream_));
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
+void Helmholtz::EnsureWorkspace(int k, int m) {
+    if (wsK_ == k && wsM_ == m) return;
+    const int64_t nk = NumUnknowns() * k;
+    dX_.Allocate(nk * sizeof(z64));
+    dX0_.Allocate(nk * sizeof(z64));
+    dW_.Allocate(nk * sizeof(z64));
+    dB_.Allocate(nk * sizeof(z64));
+    dV_.Allocate((size_t)m * nk * sizeof(z64));
+    dPartial_.Allocate((size_t)ReduceBlocks(NumUnknowns(), k) * k * sizeof(z64));
+    dScal_.Allocate((size_t)(2 * k) * sizeof(double) + (size_t)(m + 1) * k * sizeof(z64));
+    dY_.Allocate((size_t)m * k * sizeof(z64));
+    wsK_ = k;
+    wsM_ = m;
+}
+
+namespace {
+
+// lapack::ComputeGivens semantics (solve.hpp:486-487):
+// [c s; -conj(s) c] [f; g] = [rho; 0] with c real.
+void Givens(Cd f, Cd g, double& c, Cd& s, Cd& rho) {
+    const double af = std::abs(f), ag = std::abs(g);
+    if (ag == 0) { c = 1; s = 0; rho = f; return; }
+    if (af == 0) { c = 0; s = std::conj(g) / ag; rho = ag; return; }
+    const double nrm = std::hypot(af, ag);
+    c = af / nrm;
+    s = (f / af) * std::conj(g) / nrm;
+    rho = (f / af) * nrm;
+}
+
+bool AnyNaN(const std::vector<double>& v) {
+    for (double x : v)
+        if (x != x) return true;
+    return false;
+}
+
+}  // namespace
+
+void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* stats) {
+    if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    if (k < 1) throw PspError(kLogicError, "need at least one right-hand side");
+    if (m < 1) throw PspError(kLogicError, "GMRES restart length must be positive");
+    CUDA_CHECK(cudaSetDevice(device_));
+    const auto tStart = std::chrono::steady_clock::now();
+    EnsureWorkspace(k, m);
+    SolveStats local;
+    SolveStats& S = stats ? *stats : local;
+    S = SolveStats();
+    const int64_t N = NumUnknowns(), nk = N * k;
+    cudaStream_t st = stream_;
+    z64* x = dX_.as<z64>();
+    z64* x0 = dX0_.as<z64>();
+    z64* w = dW_.as<z64>();
+    z64* b = dB_.as<z64>();
+    z64* V = dV_.as<z64>();
+    double* dNorm = dScal_.as<double>();
+    double* dDelta = dNorm + k;
+    z64* dH = reinterpret_cast<z64*>(dDelta + k);
+    z64* dY = dY_.as<z64>();
+    const int nblk = ReduceBlocks(N, k);
+    const double* vel = dVel_.as<double>();
+    auto norms = [&](const z64* v, double* out) {
+        LaunchNormsPartial(v, N, k, dPartial_.as<double>(), st);
+        LaunchSumPartialReal(dPartial_.as<double>(), nblk, k, out, 1, st);
+    };
+    auto fetch = [&](void* dst, const void* src, size_t bytes) {
+        CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    };
+    cudaEvent_t e0, e1;
+    CUDA_CHECK(cudaEventCreate(&e0));
+    CUDA_CHECK(cudaEventCreate(&e1));
+    auto timed = [&](double& acc, auto&& fn) {
+        CUDA_CHECK(cudaEventRecord(e0, st));
+        fn();
+        CUDA_CHECK(cudaEventRecord(e1, st));
+        CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        acc += ms * 1e-3;
+    };
+
+    CUDA_CHECK(cudaMemcpyAsync(b, B, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
+    CUDA_CHECK(cudaMemsetAsync(x, 0, nk * sizeof(z64), st));
+    CUDA_CHECK(cudaMemcpyAsync(w, b, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
+    std::vector<double> origResid(k), beta(k), delta(k), resid(k);
+    norms(w, dNorm);
+    fetch(origResid.data(), dNorm, k * sizeof(double));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+    if (AnyNaN(origResid)) throw PspError(kRuntimeError, "Original residual norms had a NaN");
+
+    std::vector<Cd> H((size_t)k * m * m), z((size_t)k * (m + 1)), sn((size_t)k * m), y((size_t)m * k), hcol;
+    std::vector<double> cs((size_t)k * m);
+    int it = 0;
+    bool converged = false;
+    double maxRel = 0;
+    while (!converged) {
+        CUDA_CHECK(cudaMemcpyAsync(x0, x, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
+        timed(S.precondSeconds, [&] { Precondition(w, k); });
+        S.numPreconditions++;
+        norms(w, dNorm);
+        fetch(beta.data(), dNorm, k * sizeof(double));
+        CUDA_CHECK(cudaStreamSynchronize(st));
+        if (AnyNaN(beta)) throw PspError(kRuntimeError, "beta list had a NaN");
+        LaunchScaleColumns(w, dNorm, V, N, k, st);
+        std::fill(z.begin(), z.end(), Cd(0));
+        for (int r = 0; r < k; ++r) z[(size_t)r * (m + 1)] = beta[r];
+        for (int j = 0; j < m; ++j) {
+            timed(S.matvecSeconds, [&] { LaunchHelmholtzApply(V + (size_t)j * nk, w, nullptr, vel, sp_, k, st); });
+            timed(S.precondSeconds, [&] { Precondition(w, k); });
+            S.numPreconditions++;
+            const auto ta = std::chrono::steady_clock::now();
+            for (int i = 0; i <= j; ++i) {
+                LaunchMgsStep(w, i > 0 ? V + (size_t)(i - 1) * nk : nullptr, i > 0 ? dH + (size_t)(i - 1) * k : nullptr,
+                              V + (size_t)i * nk, N, k, dPartial_.as<z64>(), st);
+                LaunchSumPartialComplex(dPartial_.as<z64>(), nblk, k, dH + (size_t)i * k, st);
+            }
+            LaunchAxpyColumns(w, V + (size_t)j * nk, dH + (size_t)j * k, N, k, st);
+            norms(w, dDelta);
+            hcol.resize((size_t)(j + 1) * k);
+            fetch(hcol.data(), dH, (size_t)(j + 1) * k * sizeof(z64));
+            fetch(delta.data(), dDelta, k * sizeof(double));
+            CUDA_CHECK(cudaStreamSynchronize(st));
+            if (AnyNaN(delta)) throw PspError(kRuntimeError, "delta list had a NaN");
+            bool zeroDelta = false;
+            for (double dv : delta) zeroDelta |= (dv == 0);
+            if (zeroDelta) {
+                // solve.hpp:405-414: the reference returns here without copying
+                // the iterate back, so B keeps the right-hand sides.
+                S.luckyBreakdown = 1;
+                S.iterations = it;
+                S.finalMaxRelResid = maxRel;
+                S.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return;
+            }
+            if (j + 1 != m) LaunchScaleColumns(w, dDelta, V + (size_t)(j + 1) * nk, N, k, st);
+            for (int r = 0; r < k; ++r) {
+                Cd* Hr = &H[(size_t)r * m * m];
+                for (int i = 0; i <= j; ++i) Hr[(size_t)j * m + i] = Cd(hcol[(size_t)i * k + r]);
+                for (int i = 0; i < j; ++i) {
+                    const double c = cs[(size_t)r * m + i];
+                    const Cd s = sn[(size_t)r * m + i];
+                    const Cd a = Hr[(size_t)j * m + i], bb = Hr[(size_t)j * m + i + 1];
+                    Hr[(size_t)j * m + i] = c * a + s * bb;
+                    Hr[(size_t)j * m + i + 1] = -std::conj(s) * a + c * bb;
+                }
+                const Cd etajj = Hr[(size_t)j * m + j];
+                if (etajj != etajj) throw PspError(kRuntimeError, "H(j,j) was NaN");
+                double c;
+                Cd s, rho;
+                Givens(etajj, Cd(delta[r]), c, s, rho);
+                if (c != c || s != s || rho != rho) throw PspError(kRuntimeError, "Givens rotation had a NaN");
+                Hr[(size_t)j * m + j] = rho;
+                cs[(size_t)r * m + j] = c;
+                sn[(size_t)r * m + j] = s;
+                Cd* zr = &z[(size_t)r * (m + 1)];
+                const Cd zj = zr[j], zj1 = zr[j + 1];
+                zr[j] = c * zj + s * zj1;
+                zr[j + 1] = -std::conj(s) * zj + c * zj1;
+                for (int i = j; i >= 0; --i) {
+                    Cd acc = zr[i];
+                    for (int q = i + 1; q <= j; ++q) acc -= Hr[(size_t)q * m + i] * y[(size_t)q * k + r];
+                    y[(size_t)i * k + r] = acc / Hr[(size_t)i * m + i];
+                }
+            }
+            CUDA_CHECK(cudaMemcpyAsync(dY, y.data(), (size_t)(j + 1) * k * sizeof(z64), cudaMemcpyHostToDevice, st));
+            LaunchCombine(x0, V, nk, dY, j + 1, x, N, k, st);
+            timed(S.matvecSeconds, [&] { LaunchHelmholtzApply(x, w, b, vel, sp_, k, st); });
+            norms(w, dNorm);
+            fetch(resid.data(), dNorm, k * sizeof(double));
+            CUDA_CHECK(cudaStreamSynchronize(st));
+            S.arnoldiSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
+            if (AnyNaN(resid)) throw PspError(kRuntimeError, "resid norm list has NaN");
+            maxRel = 0;
+            for (int r = 0; r < k; ++r) maxRel = std::max(maxRel, resid[r] / origResid[r]);
+            S.history.push_back(maxRel);
+            ++it;
+            if (maxRel < relTol) {
+                converged = true;
+                break;
+            }
+            if (maxIterations_ > 0 && it >= maxIterations_) break;
+        }
+        if (maxIterations_ > 0 && it >= maxIterations_) break;
+    }
+    CUDA_CHECK(cudaMemcpyAsync(B, x, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
+    CUDA_CHECK(cudaStreamSynchronize(st));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    S.iterations = it;
+    S.converged = converged ? 1 : 0;
+    S.finalMaxRelResid = maxRel;
+    S.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+}
+
+}  // namespace psp_b200

@@ -1,0 +1,118 @@
+// DistHelmholtz on one B200: owns the device state of one Helmholtz problem
+// (PSP include/psp/dist_helmholtz.hpp:21-287).
+#pragma once
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "analysis.hpp"
+#include "kernels.cuh"
+
+namespace psp_b200 {
+
+// Device allocation owned by one object.
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { Release(); }
+    void Allocate(size_t n);
+    void Release();
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Host staging area whose arrays are uploaded in one copy; device pointers
+// are resolved after Upload().
+struct TaskArena {
+    std::vector<unsigned char> host;
+    DeviceBuffer dev;
+    template <typename T>
+    size_t Push(const std::vector<T>& v) {
+        const size_t off = (host.size() + 255) & ~size_t(255);
+        host.resize(off + v.size() * sizeof(T));
+        if (!v.empty()) std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+    void Upload(cudaStream_t st);
+    template <typename T>
+    T* At(size_t off) const { return reinterpret_cast<T*>(static_cast<unsigned char*>(dev.p) + off); }
+};
+
+struct SolveStats {
+    int iterations = 0;
+    int converged = 0;
+    int luckyBreakdown = 0;
+    double finalMaxRelResid = 0;
+    double seconds = 0;
+    double precondSeconds = 0;
+    double matvecSeconds = 0;
+    double arnoldiSeconds = 0;
+    int numPreconditions = 0;
+    std::vector<double> history;
+};
+
+struct PanelPlan;  // per class solve task lists
+
+template <typename R>
+class FactorStore;
+
+class Helmholtz {
+public:
+    Helmholtz(const DiscParams& d, double damping, int planesPerPanel, int cutoff, int device);
+    ~Helmholtz();
+
+    // Initialize(velocity) (initialize_finalize.hpp:12-377): velocity is a
+    // natural-order nx*ny*nz array on the host or (devicePtr) on the device.
+    // precision 0: complex-double fronts; 1: complex-single fronts.
+    void Initialize(const double* velocity, bool devicePtr, int panelScheme, int precision);
+    void Finalize();
+    bool Initialized() const { return initialized_; }
+
+    // Solve (solve.hpp:12-56) on a device natural-order [N][k] complex grid, in place.
+    void SolveDevice(z64* B, int k, int m, double relTol, SolveStats* stats);
+    // B := A B and B := M^{-1} B on device grids (Multiply / Precondition).
+    void MultiplyDevice(z64* B, int k);
+    void PreconditionDevice(z64* B, int k);
+    void SolvePanelDevice(z64* B, int k, int panel);
+
+    const Analysis& analysis() const { return an_; }
+    int64_t NumUnknowns() const { return (int64_t)an_.disc.nx * an_.disc.ny * an_.disc.nz; }
+    cudaStream_t stream() const { return stream_; }
+    int precision() const { return precision_; }
+    double setupSeconds() const { return setupSeconds_; }
+    int64_t factorBytes() const;
+    void SetMaxIterations(int n) { maxIterations_ = n; }
+
+    // Device tables shared with the factor stores.
+    StencilParams sp_{};
+    AssemblyParams ap_{};
+    DeviceBuffer dS1_, dS2_, dS3_, dS3a_;   // values and reciprocals back to back
+    DeviceBuffer dVel_;
+    DeviceBuffer dNdToNat_[3], dNbrRows_[3], dRel_[3];
+    std::vector<int> s3aOff_;                // per panel
+    Analysis an_;
+    double damping_;
+    int device_;
+    cudaStream_t stream_ = nullptr;
+
+private:
+    void BuildTables();
+    void Precondition(z64* B, int k);
+    void EnsureWorkspace(int k, int m);
+
+    bool initialized_ = false;
+    int precision_ = 0;
+    int maxIterations_ = 0;
+    double setupSeconds_ = 0;
+    std::unique_ptr<FactorStore<double>> f64_;
+    std::unique_ptr<FactorStore<float>> f32_;
+    // GMRES workspace
+    int wsK_ = -1, wsM_ = -1;
+    DeviceBuffer dX_, dX0_, dW_, dB_, dV_, dPartial_, dScal_, dY_;
+};
+
+}  // namespace psp_b200
