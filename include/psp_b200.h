@@ -119,6 +119,23 @@ int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info);
 /* Seconds spent in the last Initialize and bytes of stored panel factors. */
 int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* factor_bytes);
 
+/* The CUDA stream (cudaStream_t) all work of the handle is issued on. */
+int psp_cu_get_stream(const psp_cu_handle* h, void** stream);
+
+/* Kernel profiling (no counterpart in the reference, which times phases with
+ * mpi::Time): when on, every launch is bracketed by CUDA events on the
+ * handle's stream and sweeps run without graph replay.  Categories:
+ * 0 factorization GEMM, 1 panel-solve GEMM, 2 LDL diagonal blocks, 3 LDL
+ * column panels, 4 front assembly, 5 extend-add, 6 solve gathers/scatters,
+ * 7 stencil apply, 8 GMRES vector kernels, 9 whole sweeps. */
+int psp_cu_set_profiling(psp_cu_handle* h, int on);
+int psp_cu_profile_reset(psp_cu_handle* h);
+int psp_cu_profile_get(psp_cu_handle* h, int category, long long* launches, double* ms, double* flops,
+                       double* bytes);
+
+/* Algorithmic flops and bytes of one sweep for k right-hand sides. */
+int psp_cu_sweep_cost(const psp_cu_handle* h, int k, double* flops, double* bytes);
+
 /* Host-only symbolic analysis (no GPU needed): the elimination tree of panel
  * class cls (0 bottom/full inner, 1 leftover, 2 top; main.hpp:705-726) as
  * 4 ints per node (ND offset, pivot count, update count, parent) in postorder,

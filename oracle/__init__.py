@@ -180,6 +180,34 @@ class Oracle:
         return X, stats
 
 
+def sample_costs(orc, velocity, k, reps=2):
+    """Bounded timing sample of one workload (see oracle_sample in
+    psp_oracle.cpp): dict of seconds per unit of work."""
+    L = lib()
+    L.oracle_sample.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                ctypes.POINTER(ctypes.c_double)]
+    v = np.ascontiguousarray(velocity, dtype=np.float64)
+    out = np.zeros(8)
+    if L.oracle_sample(orc._h, _ptr(v), k, reps, _ptr(out)):
+        raise RuntimeError(L.oracle_last_error().decode())
+    return dict(operator=out[0], factor=[out[1], out[2], out[3]], panel_solve=[out[4], out[5], out[6]],
+                matvec=out[7])
+
+
+def modeled_rhs_per_s(orc, costs, k, iterations, restarts=1):
+    """Setup+solve and solve-only RHS/s of the oracle extrapolated from a
+    bounded sample: panels are factored one after another (threads inside
+    the fronts), each GMRES inner step costs one sweep (2P-1 panel solves)
+    and two matvecs, every restart one extra sweep."""
+    geo = orc.geometry()
+    P = geo.shape[0]
+    setup = costs["operator"] + sum(costs["factor"][c] for c in geo[:, 3])
+    sweep = sum((1 if p == P - 1 else 2) * costs["panel_solve"][geo[p, 3]] for p in range(P))
+    solve = (iterations + restarts) * sweep + 2 * iterations * costs["matvec"]
+    return dict(setup_seconds=setup, solve_seconds=solve, sweep_seconds=sweep,
+                rhs_per_s=k / (setup + solve), solve_only_rhs_per_s=k / solve)
+
+
 def num_threads():
     lib().oracle_num_threads.restype = ctypes.c_int
     return lib().oracle_num_threads()

@@ -471,6 +471,9 @@ void PartialLDL(C* F, int n, int s) {
             }
         }
         const int kStart = j0 + jb;
+        // Threads over trailing columns when not already inside a parallel
+        // region (the full factorization parallelises over panels instead).
+#pragma omp parallel for schedule(dynamic, 8) if (!omp_in_parallel() && (n - kStart) > 64)
         for (int k = kStart; k < n; ++k) {
             C* colk = F + (size_t)k * n;
             for (int j = j0; j < j0 + jb; ++j) {
@@ -1044,6 +1047,51 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
         stats->iterations = it;
         stats->converged = 1;
         stats->final_max_rel_resid = maxRel;
+        return 0;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+// Bounded timing sample of the full-size workload for the CPU baseline:
+// out[0] global operator formation, out[1+c] factorization of one panel of
+// class c (threads inside the fronts), out[4+c] one SolvePanel of that panel
+// with k right-hand sides, out[7] one Multiply with k right-hand sides.
+// Classes absent from the geometry report -1.
+int oracle_sample(void* h, const double* velocity, int k, int reps, double* out) {
+    Solver& S = *(Solver*)h;
+    try {
+        auto now = [] { return omp_get_wtime(); };
+        double t = now();
+        FormGlobalOperator(S, velocity);
+        out[0] = now() - t;
+        S.fronts.assign(S.numPanels, std::vector<Front>());
+        int rep[3] = {-1, -1, -1};
+        for (int p = S.numPanels - 1; p >= 0; --p) rep[PanelClass(S, p)] = p;
+        std::vector<C> B((size_t)S.N * k);
+        uint64_t seed = 12345;
+        for (auto& v : B) {
+            seed = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+            const double a = ((seed >> 11) & 0xFFFFF) / double(0xFFFFF) - 0.5;
+            const double b = ((seed >> 33) & 0xFFFFF) / double(0xFFFFF) - 0.5;
+            v = C(a, b);
+        }
+        for (int c = 0; c < 3; ++c) {
+            out[1 + c] = -1;
+            out[4 + c] = -1;
+            if (rep[c] < 0) continue;
+            t = now();
+            FactorPanel(S, rep[c], velocity);
+            out[1 + c] = now() - t;
+            t = now();
+            for (int r = 0; r < reps; ++r) SolvePanel(S, B.data(), k, rep[c]);
+            out[4 + c] = (now() - t) / std::max(reps, 1);
+            std::vector<Front>().swap(S.fronts[rep[c]]);
+        }
+        t = now();
+        Multiply(S, B.data(), k);
+        out[7] = now() - t;
         return 0;
     } catch (std::exception& e) {
         g_err = e.what();

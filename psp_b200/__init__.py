@@ -69,8 +69,12 @@ C_ABI_SYMBOLS = [
     "psp_cu_last_error", "psp_cu_create", "psp_cu_destroy", "psp_cu_initialize", "psp_cu_initialize_device",
     "psp_cu_solve", "psp_cu_solve_device", "psp_cu_finalize", "psp_cu_multiply", "psp_cu_precondition",
     "psp_cu_multiply_device", "psp_cu_precondition_device", "psp_cu_solve_panel", "psp_cu_set_max_iterations",
-    "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class",
+    "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class", "psp_cu_get_stream",
+    "psp_cu_set_profiling", "psp_cu_profile_reset", "psp_cu_profile_get", "psp_cu_sweep_cost",
 ]
+
+PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
+                      "gather_scatter", "stencil", "gmres_vector", "sweep"]
 
 _lib = None
 
@@ -104,6 +108,11 @@ def lib():
         L.psp_cu_setup_info.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong)]
         L.psp_cu_analyze_class.argtypes = [ctypes.POINTER(_Disc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            ip, ip, ip, ip]
+        L.psp_cu_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.psp_cu_set_profiling.argtypes = [vp, ctypes.c_int]
+        L.psp_cu_profile_reset.argtypes = [vp]
+        L.psp_cu_profile_get.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp]
+        L.psp_cu_sweep_cost.argtypes = [vp, ctypes.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -327,6 +336,34 @@ class DistHelmholtz:
     def solve_panel(self, B, p):
         """B := T_p B on panel p only (SolvePanel, solve.hpp:736-882) on a copy."""
         return self._grid_op(lib().psp_cu_solve_panel, B, int(p))
+
+    def stream_ptr(self):
+        """The cudaStream_t the handle issues all work on (as an int)."""
+        s = ctypes.c_void_p()
+        _check(lib().psp_cu_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def set_profiling(self, on):
+        _check(lib().psp_cu_set_profiling(self._h, 1 if on else 0))
+
+    def profile_reset(self):
+        _check(lib().psp_cu_profile_reset(self._h))
+
+    def profile(self):
+        """Per-category {launches, ms, flops, bytes} of profiled launches."""
+        out = {}
+        for i, name in enumerate(PROFILE_CATEGORIES):
+            n = ctypes.c_longlong()
+            ms, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            _check(lib().psp_cu_profile_get(self._h, i, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(fl),
+                                            ctypes.byref(by)))
+            out[name] = dict(launches=n.value, ms=ms.value, flops=fl.value, bytes=by.value)
+        return out
+
+    def sweep_cost(self, k):
+        f, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().psp_cu_sweep_cost(self._h, int(k), ctypes.byref(f), ctypes.byref(b)))
+        return f.value, b.value
 
     def multiply_device(self, B):
         _check(lib().psp_cu_multiply_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))

@@ -190,6 +190,48 @@ int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info) {
     return PSP_CU_OK;
 }
 
+int psp_cu_get_stream(const psp_cu_handle* h, void** stream) {
+    if (int e = CheckHandle(h)) return e;
+    if (stream) *stream = (void*)h->solver->stream();
+    return PSP_CU_OK;
+}
+
+int psp_cu_set_profiling(psp_cu_handle* h, int on) {
+    if (int e = CheckHandle(h)) return e;
+    h->solver->profiler().enabled = on != 0;
+    return PSP_CU_OK;
+}
+
+int psp_cu_profile_reset(psp_cu_handle* h) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->profiler().Reset(); });
+}
+
+int psp_cu_profile_get(psp_cu_handle* h, int category, long long* launches, double* ms, double* flops,
+                       double* bytes) {
+    if (int e = CheckHandle(h)) return e;
+    if (category < 0 || category >= psp_b200::kProfNumCategories) {
+        g_lastError = "profile category out of range";
+        return PSP_CU_LOGIC_ERROR;
+    }
+    return Guard([&] {
+        psp_b200::Profiler& p = h->solver->profiler();
+        p.Flush();
+        const psp_b200::ProfileTotals& t = p.totals[category];
+        if (launches) *launches = t.launches;
+        if (ms) *ms = t.ms;
+        if (flops) *flops = t.flops;
+        if (bytes) *bytes = t.bytes;
+    });
+}
+
+int psp_cu_sweep_cost(const psp_cu_handle* h, int k, double* flops, double* bytes) {
+    if (int e = CheckHandle(h)) return e;
+    if (flops) *flops = h->solver->SweepFlops(k);
+    if (bytes) *bytes = h->solver->SweepBytes(k);
+    return PSP_CU_OK;
+}
+
 int psp_cu_analyze_class(const psp_cu_disc* disc, int planes_per_panel, int cutoff, int cls, int* num_nodes,
                          int* vsize, int* info, int* nd_to_nat) {
     if (!disc) {

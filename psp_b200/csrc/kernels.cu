@@ -34,17 +34,6 @@ __device__ __forceinline__ Terms StencilAt(const StencilParams& sp, int x, int y
     return t;
 }
 
-// z-coupling of a global row to its v-1 / v+1 neighbour (the -vTermL/-vTermR
-// entries of FormGlobalRow); only PML tables are involved.
-__device__ __forceinline__ z64 CouplingBelow(const StencilParams& sp, int x, int y, int v) {
-    const z64 cz = sp.s1[x + 1] * sp.s2[y + 1];
-    return sp.ihz2 * (cz * (sp.is3[v] + sp.is3[v + 1]));
-}
-__device__ __forceinline__ z64 CouplingAbove(const StencilParams& sp, int x, int y, int v) {
-    const z64 cz = sp.s1[x + 1] * sp.s2[y + 1];
-    return sp.ihz2 * (cz * (sp.is3[v + 2] + sp.is3[v + 1]));
-}
-
 // ---------------------------------------------------------------- stencil apply
 
 constexpr int kApplyTX = 64;
@@ -318,132 +307,6 @@ __global__ void __launch_bounds__(kThreads) ldl_trsm_kernel(const FactorFront<R>
     }
 }
 
-// ---------------------------------------------------------------- panel solves
-
-template <typename R>
-__device__ __forceinline__ cpx<R> LoadPanelRhs(const PanelIO& io, const z64* __restrict__ B, int col, int r) {
-    const int pn = io.ndToNat[col];
-    const int xy = pn % io.nxy, vl = pn / io.nxy;
-    if (vl < io.padding) return mk<R>(0, 0);
-    const int v = io.vOffset + vl;
-    const int64_t nat = xy + (int64_t)(io.nz - 1 - v) * io.nxy;
-    const int x = xy % io.nx, y = xy / io.nx;
-    if (io.inMode == 2) {
-        if (v != io.highV) return mk<R>(0, 0);
-        const z64 val = CouplingAbove(io.sp, x, y, v) * B[(nat - io.nxy) * io.ldk + r];
-        return ccast<R>(val);
-    }
-    z64 val = B[nat * io.ldk + r];
-    if (io.inMode == 1 && v == io.lowV) val += CouplingBelow(io.sp, x, y, v) * B[(nat + io.nxy) * io.ldk + r];
-    return ccast<R>(val);
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads) fwd_gather_kernel(const SolveFront<R>* __restrict__ fr,
-                                                              const int2* __restrict__ tasks,
-                                                              const z64* __restrict__ B, int k, PanelIO io) {
-    extern __shared__ unsigned char smem_raw[];
-    cpx<R>* acc = reinterpret_cast<cpx<R>*>(smem_raw);  // [kSolveRowTile][k] column-major
-    __shared__ int range[2][2];
-    const int2 task = tasks[blockIdx.x];
-    const SolveFront<R> f = fr[task.x];
-    const int i0 = task.y;
-    const int rows = min(kSolveRowTile, f.s + f.u - i0);
-    const int tid = threadIdx.x;
-    for (int e = tid; e < rows * k; e += blockDim.x) {
-        const int i = e % rows, r = e / rows;
-        const int gi = i0 + i;
-        acc[i + r * kSolveRowTile] = (gi < f.s) ? LoadPanelRhs<R>(io, B, f.ndOff + gi, r) : mk<R>(0, 0);
-    }
-    if (tid < 2) {
-        const int c = tid == 0 ? f.child0 : f.child1;
-        int a0 = 0, a1 = 0;
-        if (c >= 0) {
-            const int* rel = fr[c].rel;
-            const int uc = fr[c].u;
-            int lo = 0, hi = uc;
-            while (lo < hi) { const int mid = (lo + hi) / 2; if (rel[mid] < i0) lo = mid + 1; else hi = mid; }
-            a0 = lo;
-            hi = uc;
-            while (lo < hi) { const int mid = (lo + hi) / 2; if (rel[mid] < i0 + rows) lo = mid + 1; else hi = mid; }
-            a1 = lo;
-        }
-        range[tid][0] = a0;
-        range[tid][1] = a1;
-    }
-    __syncthreads();
-    for (int ci = 0; ci < 2; ++ci) {
-        const int c = ci == 0 ? f.child0 : f.child1;
-        if (c < 0) continue;
-        const int a0 = range[ci][0], n = range[ci][1] - a0;
-        const SolveFront<R> ch = fr[c];
-        const int64_t ldc = ch.s + ch.u;
-        for (int e = tid; e < n * k; e += blockDim.x) {
-            const int a = a0 + e % n, r = e / n;
-            acc[(ch.rel[a] - i0) + r * kSolveRowTile] += ch.Ov[ch.s + a + r * ldc];
-        }
-        __syncthreads();
-    }
-    const int64_t ld = f.s + f.u;
-    for (int e = tid; e < rows * k; e += blockDim.x) {
-        const int i = e % rows, r = e / rows;
-        const int gi = i0 + i;
-        const cpx<R> v = acc[i + r * kSolveRowTile];
-        if (gi < f.s) {
-            f.Rv[gi + r * ld] = v;
-            f.Ov[gi + r * ld] = mk<R>(0, 0);
-        } else {
-            f.Ov[gi + r * ld] = v;
-        }
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads) bwd_gather_kernel(const SolveFront<R>* __restrict__ fr,
-                                                              const int2* __restrict__ tasks, int k) {
-    const int2 task = tasks[blockIdx.x];
-    const SolveFront<R> f = fr[task.x];
-    const int i0 = task.y;
-    const int rows = min(kSolveRowTile, f.s + f.u - i0);
-    const int64_t ld = f.s + f.u;
-    for (int e = threadIdx.x; e < rows * k; e += blockDim.x) {
-        const int i = e % rows, r = e / rows;
-        const int gi = i0 + i;
-        if (gi < f.s) {
-            cpx<R>* p = f.Ov + gi + r * ld;
-            *p = cdiv(*p, f.D[gi]);
-        } else {
-            const SolveFront<R> p = fr[f.parent];
-            const int pr = f.rel[gi - f.s];
-            const int64_t ldp = p.s + p.u;
-            f.Ov[gi + r * ld] = pr < p.s ? p.Rv[pr + r * ldp] : p.Ov[pr + r * ldp];
-        }
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kThreads) scatter_kernel(const SolveFront<R>* __restrict__ fr,
-                                                           const int2* __restrict__ tasks, z64* __restrict__ B,
-                                                           int k, PanelIO io) {
-    const int2 task = tasks[blockIdx.x];
-    const SolveFront<R> f = fr[task.x];
-    const int i0 = task.y;
-    const int rows = min(kSolveRowTile, f.s - i0);
-    const int64_t ld = f.s + f.u;
-    for (int e = threadIdx.x; e < rows * k; e += blockDim.x) {
-        const int i = e % rows, r = e / rows;
-        const int gi = i0 + i;
-        const int pn = io.ndToNat[f.ndOff + gi];
-        const int xy = pn % io.nxy, vl = pn / io.nxy;
-        if (vl < io.padding) continue;
-        const int v = io.vOffset + vl;
-        const int64_t nat = xy + (int64_t)(io.nz - 1 - v) * io.nxy;
-        const z64 val = ccast<double>(f.Rv[gi + r * ld]);
-        z64* dst = B + nat * io.ldk + r;
-        *dst = io.outAccumulate ? (*dst + val) : val;
-    }
-}
-
 // ---------------------------------------------------------------- GMRES vectors
 
 constexpr int kReduceMaxBlocks = 1184;  // 8 per SM on 148 SMs
@@ -613,35 +476,6 @@ void LaunchLdlTrsm(const FactorFront<R>* fronts, const int2* tasks, int n, int J
     CUDA_LAUNCH_CHECK();
 }
 
-template <typename R>
-void LaunchForwardGather(const SolveFront<R>* fr, const int2* tasks, int n, const z64* B, int k, PanelIO io,
-                         cudaStream_t st) {
-    if (n <= 0) return;
-    const size_t smem = sizeof(cpx<R>) * kSolveRowTile * k;
-    static bool attr = false;
-    if (!attr) {
-        CUDA_CHECK(cudaFuncSetAttribute(fwd_gather_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(sizeof(cpx<R>) * kSolveRowTile * 64)));
-        attr = true;
-    }
-    fwd_gather_kernel<R><<<n, kThreads, smem, st>>>(fr, tasks, B, k, io);
-    CUDA_LAUNCH_CHECK();
-}
-
-template <typename R>
-void LaunchBackwardGather(const SolveFront<R>* fr, const int2* tasks, int n, int k, cudaStream_t st) {
-    if (n <= 0) return;
-    bwd_gather_kernel<R><<<n, kThreads, 0, st>>>(fr, tasks, k);
-    CUDA_LAUNCH_CHECK();
-}
-
-template <typename R>
-void LaunchScatter(const SolveFront<R>* fr, const int2* tasks, int n, z64* B, int k, PanelIO io, cudaStream_t st) {
-    if (n <= 0) return;
-    scatter_kernel<R><<<n, kThreads, 0, st>>>(fr, tasks, B, k, io);
-    CUDA_LAUNCH_CHECK();
-}
-
 int ReduceBlocks(int64_t npoints, int k) {
     const dim3 bd = ReduceBlockDim(k);
     return (int)std::max<int64_t>(1, std::min<int64_t>(CeilDiv(npoints, bd.y), kReduceMaxBlocks));
@@ -697,11 +531,7 @@ void LaunchAxpyColumns(z64* w, const z64* v, const z64* h, int64_t npoints, int 
                                     cudaStream_t);                                                             \
     template void LaunchExtendAdd<R>(const FactorFront<R>*, const int2*, int, cudaStream_t);                   \
     template void LaunchLdlDiag<R>(const FactorFront<R>*, const int*, int, int, int*, cudaStream_t);           \
-    template void LaunchLdlTrsm<R>(const FactorFront<R>*, const int2*, int, int, cudaStream_t);                \
-    template void LaunchForwardGather<R>(const SolveFront<R>*, const int2*, int, const z64*, int, PanelIO,     \
-                                         cudaStream_t);                                                        \
-    template void LaunchBackwardGather<R>(const SolveFront<R>*, const int2*, int, int, cudaStream_t);          \
-    template void LaunchScatter<R>(const SolveFront<R>*, const int2*, int, z64*, int, PanelIO, cudaStream_t);
+    template void LaunchLdlTrsm<R>(const FactorFront<R>*, const int2*, int, int, cudaStream_t);
 
 PSP_INSTANTIATE(double)
 PSP_INSTANTIATE(float)

@@ -108,15 +108,40 @@ void LaunchLdlTrsm(const FactorFront<R>* fronts, const int2* tasks, int n, int J
 
 // ------------------------------------------------------------------ panel solves
 
-// One front of the panel being solved (cliq::Solve replacement).
+// One front of the panel being solved (cliq::Solve replacement, sweep.cu).
 template <typename R>
-struct SolveFront {
-    const cpx<R>* G;
-    const cpx<R>* D;
-    cpx<R>* Rv;      // (s+u) x k work vector, ld = s+u
-    cpx<R>* Ov;      // (s+u) x k work vector, ld = s+u
-    const int* rel;
-    int s, u, ndOff, parent, child0, child1;
+struct SweepFront {
+    const cpx<R>* G;      // (s+u) x s selectively inverted factor, ld = s+u
+    const cpx<R>* D;      // pivots
+    cpx<R>* Rb;           // [s+u][3][k]: natural rhs, child 0 update, child 1 update
+    cpx<R>* parentRb;     // the parent's Rb (null for a root)
+    cpx<R>* Y;            // [s][k] forward result
+    cpx<R>* Z;            // [s+u][k] backward input
+    const int* lower;     // u ND indices of the front's structure
+    const int* rel;       // u rows of the structure in the parent front
+    int s, u, ndOff, childSlot;
+};
+
+// One CTA of a sweep launch: kSweepRows output rows from row0, kSweepCols
+// right-hand sides from col0, the K-chunk [k0, k1); split `split` of `nsplit`
+// whose partials live at slot+split and whose arrival counter is `counter`.
+struct SweepTile {
+    int front, row0, col0, k0, k1, split, nsplit, slot, counter;
+};
+
+constexpr int kSweepRows = 64;     // output rows per CTA (one per thread of a slice)
+constexpr int kSweepSlices = 4;    // K-slices per CTA, one warp pair each
+constexpr int kSweepThreads = kSweepRows * kSweepSlices;
+constexpr int kSweepCols = 16;
+constexpr size_t kSweepSmemBytes = 32 * 1024;  // staged right-hand-side chunk
+
+// Device scratch of the sweep: split-K partials (kSweepRows*kSweepCols
+// complex entries per slot), arrival counters (zero between launches) and the
+// panel's ND-ordered solution vector [ND index][k].
+struct SweepWork {
+    void* partials;
+    int* counters;
+    void* xnd;
 };
 
 struct PanelIO {
@@ -131,14 +156,25 @@ struct PanelIO {
     StencilParams sp;
 };
 
+// Largest K-chunk a sweep CTA can stage.
 template <typename R>
-void LaunchForwardGather(const SolveFront<R>* fr, const int2* tasks, int n, const z64* B, int k, PanelIO io,
-                         cudaStream_t st);
+int SweepMaxChunk();
+// Sets kernel attributes the sweep kernels need (call before any graph capture).
 template <typename R>
-void LaunchBackwardGather(const SolveFront<R>* fr, const int2* tasks, int n, int k, cudaStream_t st);
+void PrepareSweepKernels();
+// tasks: (front, first row), kSweepRows rows each
 template <typename R>
-void LaunchScatter(const SolveFront<R>* fr, const int2* tasks, int n, z64* B, int k, PanelIO io, cudaStream_t st);
-constexpr int kSolveRowTile = 64;
+void LaunchSweepPregather(const SweepFront<R>* fr, const int2* tasks, int n, const z64* B, int k, const PanelIO& io,
+                          cudaStream_t st);
+template <typename R>
+void LaunchSweepForward(const SweepFront<R>* fr, const SweepTile* tiles, int n, int maxChunk, int k,
+                        const SweepWork& w, cudaStream_t st);
+template <typename R>
+void LaunchSweepBackwardGather(const SweepFront<R>* fr, const int2* tasks, int n, int k, const SweepWork& w,
+                               cudaStream_t st);
+template <typename R>
+void LaunchSweepBackward(const SweepFront<R>* fr, const SweepTile* tiles, int n, int maxChunk, z64* B, int k,
+                         const PanelIO& io, const SweepWork& w, cudaStream_t st);
 
 // ------------------------------------------------------------------ GMRES vectors
 

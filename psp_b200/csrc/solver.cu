@@ -67,6 +67,48 @@ void UploadVector(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t st) {
     CUDA_CHECK(cudaStreamSynchronize(st));
 }
 
+// Sum over r < M of the nonzero products in row r of a triangular operand.
+double TriRowSum(int64_t M, int64_t K, int tri) {
+    if (tri == 1) {  // k <= r
+        if (M <= K) return (double)M * (M + 1) / 2;
+        return (double)K * (K + 1) / 2 + (double)(M - K) * K;
+    }
+    if (tri == 2) {  // k >= r
+        const int64_t m = std::min(M, K);
+        return (double)m * K - (double)m * (m - 1) / 2;
+    }
+    return (double)M * K;
+}
+
+// Algorithmic real flops (8 per complex multiply-add, structural zeros
+// skipped) and algorithmic bytes (nonzero operand elements read once, output
+// written once and read once when accumulated) of one batched-GEMM op.
+template <typename R>
+void OpCost(const GemmOp<R>& op, double& flops, double& bytes) {
+    double macs, aElems, bElems = (double)op.K * op.N, cElems;
+    if (op.lowerC) {
+        cElems = (double)op.N * op.M - (double)op.N * (op.N - 1) / 2;
+        macs = cElems * op.K;
+        aElems = (double)op.M * op.K;
+    } else if (op.triA) {
+        aElems = TriRowSum(op.M, op.K, op.triA);
+        macs = aElems * op.N;
+        cElems = (double)op.M * op.N;
+    } else if (op.triB) {
+        bElems = TriRowSum(op.N, op.K, op.triB == 1 ? 2 : 1);
+        macs = bElems * op.M;
+        aElems = (double)op.M * op.K;
+        cElems = (double)op.M * op.N;
+    } else {
+        macs = (double)op.M * op.N * op.K;
+        aElems = (double)op.M * op.K;
+        cElems = (double)op.M * op.N;
+    }
+    const bool acc = op.beta_re != R(0) || op.beta_im != R(0);
+    flops += 8.0 * macs;
+    bytes += sizeof(cpx<R>) * (aElems + bElems + cElems * (acc ? 2 : 1));
+}
+
 template <typename R>
 GemmOp<R> MakeOp(const cpx<R>* A, int64_t lda, int transA, const cpx<R>* B, int64_t ldb, int transB, cpx<R>* C,
                  int64_t ldc, int M, int N, int K, R alpha, R beta) {
@@ -90,11 +132,18 @@ GemmOp<R> MakeOp(const cpx<R>* A, int64_t lda, int transA, const cpx<R>* B, int6
 template <typename R>
 class FactorStore {
 public:
-    explicit FactorStore(Helmholtz& h) : h_(h), an_(h.an_) {}
+    explicit FactorStore(Helmholtz& h) : h_(h), an_(h.an_) { PrepareSweepKernels<R>(); }
+    ~FactorStore() {
+        for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
+    }
     void Factor();
     void SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc);
-    void Sweep(z64* B, int ldk, int k);
+    // One sweep (Precondition); replayed from a captured CUDA graph when
+    // `useGraph` and profiling is off.
+    void Sweep(z64* B, int ldk, int k, bool useGraph);
     int64_t Bytes() const { return (int64_t)(G_.bytes + D_.bytes); }
+    double SweepFlops(int k) const;
+    double SweepBytes(int k) const;
 
 private:
     struct Step {
@@ -102,7 +151,15 @@ private:
         size_t a = 0, b = 0;
         int n = 0, J = 0;
         size_t bytes = 0;
+        double flops = 0, abytes = 0;
     };
+    struct SweepGraph {
+        z64* B;
+        int ldk, k;
+        cudaGraphExec_t exec;
+    };
+    std::vector<SweepGraph> graphs_;
+    void SweepEager(z64* B, int ldk, int k);
     void FactorGroup(int p0, int p1, FactorFront<R>* hostFronts, std::vector<FactorFront<R>>& all);
     void BuildSolvePlan(int k);
 
@@ -115,15 +172,16 @@ private:
     DeviceBuffer status_;
     // solve plan for one RHS block width
     int planK_ = -1;
-    DeviceBuffer Rv_, Ov_;
+    DeviceBuffer Rb_, Y_, Z_, Xnd_, partials_, counters_;
     TaskArena solveArena_;
     struct ClassPlan {
-        std::vector<size_t> fg, fTiles, bTiles;
-        std::vector<int> fgN, fTilesN, bTilesN;
-        size_t sc = 0;
-        int scN = 0;
+        size_t pre = 0;
+        int preN = 0;
+        std::vector<size_t> fTiles, bTiles, bGather;
+        std::vector<int> fN, bN, bGatherN, fChunk, bChunk;
+        std::vector<double> fFlops, fBytes, bFlops, bBytes;
     } cplan_[3];
-    std::vector<size_t> panelFronts_, panelFwdOps_, panelBwdOps_;
+    std::vector<size_t> panelFronts_;
 };
 
 template <typename R>
@@ -256,6 +314,7 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
         if (tiles.empty()) { ops.clear(); return; }
         Step s;
         s.kind = Step::kGemm;
+        for (const GemmOp<R>& op : ops) OpCost(op, s.flops, s.abytes);
         s.a = arenaTasks.Push(ops);
         s.b = arenaTasks.Push(tiles);
         s.n = (int)tiles.size();
@@ -398,21 +457,31 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
             case Step::kMemset:
                 if (s.bytes) CUDA_CHECK(cudaMemsetAsync((char*)arena.p + s.a, 0, s.bytes, st));
                 break;
-            case Step::kAssemble:
+            case Step::kAssemble: {
+                ProfScope ps(st, kProfAssemble);
                 LaunchAssemble<R>(dFronts, arenaTasks.At<int>(s.a), s.n, h_.ap_, st);
                 break;
-            case Step::kExtend:
+            }
+            case Step::kExtend: {
+                ProfScope ps(st, kProfExtendAdd);
                 LaunchExtendAdd<R>(dFronts, arenaTasks.At<int2>(s.a), s.n, st);
                 break;
-            case Step::kDiag:
+            }
+            case Step::kDiag: {
+                ProfScope ps(st, kProfLdlDiag);
                 LaunchLdlDiag<R>(dFronts, arenaTasks.At<int>(s.a), s.n, s.J, status_.as<int>(), st);
                 break;
-            case Step::kTrsm:
+            }
+            case Step::kTrsm: {
+                ProfScope ps(st, kProfLdlTrsm);
                 LaunchLdlTrsm<R>(dFronts, arenaTasks.At<int2>(s.a), s.n, s.J, st);
                 break;
-            case Step::kGemm:
+            }
+            case Step::kGemm: {
+                ProfScope ps(st, kProfFactorGemm, s.flops, s.abytes);
                 LaunchGemm<R>(arenaTasks.At<GemmOp<R>>(s.a), arenaTasks.At<GemmTile>(s.b), s.n, kGemmSquare, st);
                 break;
+            }
         }
     }
     CUDA_CHECK(cudaStreamSynchronize(st));
@@ -425,84 +494,139 @@ void FactorStore<R>::BuildSolvePlan(int k) {
     const XYTree& tree = an_.tree;
     const int np = g.numPanels;
     const int nd = (int)depthNodes_.size();
-    std::vector<std::vector<int64_t>> vecOff(3);
-    int64_t maxVec = 0;
+    // Work vectors per class: R planes (3 (s+u) k), Y (s k) and Z ((s+u) k).
+    std::vector<std::vector<int64_t>> rOff(3), yOff(3), zOff(3);
+    int64_t maxR = 0, maxY = 0, maxZ = 0;
+    int maxSub = 0;
     for (int c = 0; c < 3; ++c) {
         if (!an_.classUsed[c]) continue;
         const ClassStructure& cs = an_.cls[c];
-        vecOff[c].resize(nn_);
-        int64_t tot = 0;
+        rOff[c].resize(nn_); yOff[c].resize(nn_); zOff[c].resize(nn_);
+        int64_t tr = 0, ty = 0, tz = 0;
         for (int t = 0; t < nn_; ++t) {
-            vecOff[c][t] = tot;
-            tot += (int64_t)(cs.size[t] + cs.usize[t]) * k;
+            rOff[c][t] = tr; yOff[c][t] = ty; zOff[c][t] = tz;
+            tr += (int64_t)(cs.size[t] + cs.usize[t]) * 3 * k;
+            ty += (int64_t)cs.size[t] * k;
+            tz += (int64_t)(cs.size[t] + cs.usize[t]) * k;
         }
-        maxVec = std::max(maxVec, tot);
+        maxR = std::max(maxR, tr); maxY = std::max(maxY, ty); maxZ = std::max(maxZ, tz);
+        maxSub = std::max(maxSub, cs.nSub);
     }
-    Rv_.Allocate(maxVec * sizeof(cpx<R>));
-    Ov_.Allocate(maxVec * sizeof(cpx<R>));
+    Rb_.Allocate(maxR * sizeof(cpx<R>));
+    Y_.Allocate(maxY * sizeof(cpx<R>));
+    Z_.Allocate(maxZ * sizeof(cpx<R>));
+    Xnd_.Allocate((size_t)maxSub * k * sizeof(cpx<R>));
     solveArena_.host.clear();
     panelFronts_.assign(np, 0);
-    panelFwdOps_.assign(np, 0);
-    panelBwdOps_.assign(np, 0);
     for (int p = 0; p < np; ++p) {
         const int c = g.Class(p);
         const ClassStructure& cs = an_.cls[c];
-        std::vector<SolveFront<R>> fr(nn_);
-        std::vector<GemmOp<R>> fo(nn_), bo(nn_);
+        std::vector<SweepFront<R>> fr(nn_);
         for (int t = 0; t < nn_; ++t) {
-            SolveFront<R>& f = fr[t];
+            SweepFront<R>& f = fr[t];
             const XYNode& node = tree.nodes[t];
             f.G = G_.as<cpx<R>>() + gOff_[(size_t)p * nn_ + t];
             f.D = D_.as<cpx<R>>() + dOff_[(size_t)p * nn_ + t];
-            f.Rv = Rv_.as<cpx<R>>() + vecOff[c][t];
-            f.Ov = Ov_.as<cpx<R>>() + vecOff[c][t];
+            f.Rb = Rb_.as<cpx<R>>() + rOff[c][t];
+            f.parentRb = node.parent >= 0 ? Rb_.as<cpx<R>>() + rOff[c][node.parent] : nullptr;
+            f.Y = Y_.as<cpx<R>>() + yOff[c][t];
+            f.Z = Z_.as<cpx<R>>() + zOff[c][t];
+            f.lower = h_.dLower_[c].as<int>() + cs.lowerOff[t];
             f.rel = h_.dRel_[c].as<int>() + cs.lowerOff[t];
             f.s = cs.size[t];
             f.u = cs.usize[t];
             f.ndOff = cs.off[t];
-            f.parent = node.parent;
-            f.child0 = node.numChildren > 0 ? node.child[0] : -1;
-            f.child1 = node.numChildren > 1 ? node.child[1] : -1;
-            const int64_t ld = f.s + f.u;
-            fo[t] = MakeOp<R>(f.G, ld, 0, f.Rv, ld, 0, f.Ov, ld, f.s + f.u, k, f.s, R(1), R(1));
-            fo[t].triA = 1;
-            bo[t] = MakeOp<R>(f.G, ld, 1, f.Ov, ld, 0, f.Rv, ld, f.s, k, f.s + f.u, R(1), R(0));
-            bo[t].triA = 2;
+            f.childSlot = (node.parent >= 0 && tree.nodes[node.parent].child[1] == t) ? 1 : 0;
         }
         panelFronts_[p] = solveArena_.Push(fr);
-        panelFwdOps_[p] = solveArena_.Push(fo);
-        panelBwdOps_[p] = solveArena_.Push(bo);
     }
+    // Tiles of one depth and direction.  The K-chunk shrinks until the launch
+    // has a few CTAs per SM; rows of a tile share one K range (inv(L11) is
+    // triangular, so the forward range stops at the tile's last row and the
+    // backward range starts at its first).
+    const int maxChunk = SweepMaxChunk<R>();
+    int64_t maxSlots = 1, maxCounters = 1;
+    auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepTile>& tiles, int& chunk,
+                         double& flops, double& bytes) {
+        auto build = [&](int kc, bool emit) {
+            int64_t n = 0, slots = 0, counters = 0;
+            for (int t : depthNodes_[d]) {
+                const int s = cs.size[t], u = cs.usize[t];
+                const int M = fwd ? s + u : s, K = fwd ? s : s + u;
+                for (int col0 = 0; col0 < k; col0 += kSweepCols)
+                    for (int row0 = 0; row0 < M; row0 += kSweepRows) {
+                        const int kb = fwd ? 0 : row0;
+                        const int ke = fwd ? std::min(K, row0 + kSweepRows) : K;
+                        const int ns = std::max(1, (int)CeilDiv(ke - kb, kc));
+                        for (int sp = 0; sp < ns; ++sp) {
+                            if (emit) {
+                                SweepTile tl;
+                                tl.front = t; tl.row0 = row0; tl.col0 = col0;
+                                tl.k0 = kb + sp * kc;
+                                tl.k1 = std::min(ke, kb + (sp + 1) * kc);
+                                tl.split = sp; tl.nsplit = ns;
+                                tl.slot = ns > 1 ? (int)slots : -1;
+                                tl.counter = ns > 1 ? (int)counters : -1;
+                                tiles.push_back(tl);
+                            }
+                            ++n;
+                        }
+                        if (ns > 1) { slots += ns; ++counters; }
+                    }
+            }
+            if (emit) {
+                maxSlots = std::max(maxSlots, slots);
+                maxCounters = std::max(maxCounters, counters);
+            }
+            return n;
+        };
+        int kc = maxChunk;
+        while (kc > 64 && build(kc, false) < 2 * 148) kc /= 2;
+        build(kc, true);
+        chunk = kc;
+        // longest K ranges first, so the launch does not end on a long tail
+        std::stable_sort(tiles.begin(), tiles.end(), [](const SweepTile& a, const SweepTile& b) {
+            return (a.k1 - a.k0) > (b.k1 - b.k0);
+        });
+        for (int t : depthNodes_[d]) {
+            const double s = cs.size[t], u = cs.usize[t];
+            const double nz = (s + u) * s - s * (s - 1) / 2;  // nonzeros of G
+            flops += 8.0 * nz * k;
+            bytes += sizeof(cpx<R>) * (nz + (fwd ? (s + 2 * (s + u)) : (2 * (s + u) + 2 * s)) * k);
+        }
+    };
     for (int c = 0; c < 3; ++c) {
         if (!an_.classUsed[c]) continue;
         const ClassStructure& cs = an_.cls[c];
         ClassPlan& cp = cplan_[c];
-        cp.fg.assign(nd, 0); cp.fTiles.assign(nd, 0); cp.bTiles.assign(nd, 0);
-        cp.fgN.assign(nd, 0); cp.fTilesN.assign(nd, 0); cp.bTilesN.assign(nd, 0);
+        cp.fTiles.assign(nd, 0); cp.bTiles.assign(nd, 0); cp.bGather.assign(nd, 0);
+        cp.fN.assign(nd, 0); cp.bN.assign(nd, 0); cp.bGatherN.assign(nd, 0);
+        cp.fChunk.assign(nd, 0); cp.bChunk.assign(nd, 0);
+        cp.fFlops.assign(nd, 0); cp.fBytes.assign(nd, 0); cp.bFlops.assign(nd, 0); cp.bBytes.assign(nd, 0);
+        std::vector<int2> pre;
         for (int d = 0; d < nd; ++d) {
-            std::vector<int2> gt;
-            std::vector<GemmTile> ft, bt;
-            for (int t : depthNodes_[d]) {
-                const int s = cs.size[t], u = cs.usize[t];
-                for (int i0 = 0; i0 < s + u; i0 += kSolveRowTile) gt.push_back(make_int2(t, i0));
-                GemmOp<R> fo = MakeOp<R>(nullptr, 1, 0, nullptr, 1, 0, nullptr, 1, s + u, k, s, R(1), R(1));
-                GemmOp<R> bo = MakeOp<R>(nullptr, 1, 1, nullptr, 1, 0, nullptr, 1, s, k, s + u, R(1), R(0));
-                AppendGemmTiles(fo, t, kGemmSkinny, ft);
-                AppendGemmTiles(bo, t, kGemmSkinny, bt);
-            }
-            cp.fg[d] = solveArena_.Push(gt);
-            cp.fgN[d] = (int)gt.size();
+            std::vector<SweepTile> ft, bt;
+            std::vector<int2> bg;
+            makeTiles(cs, d, true, ft, cp.fChunk[d], cp.fFlops[d], cp.fBytes[d]);
+            makeTiles(cs, d, false, bt, cp.bChunk[d], cp.bFlops[d], cp.bBytes[d]);
+            for (int t : depthNodes_[d])
+                for (int i0 = 0; i0 < cs.size[t] + cs.usize[t]; i0 += kSweepRows) {
+                    bg.push_back(make_int2(t, i0));
+                    pre.push_back(make_int2(t, i0));
+                }
             cp.fTiles[d] = solveArena_.Push(ft);
-            cp.fTilesN[d] = (int)ft.size();
+            cp.fN[d] = (int)ft.size();
             cp.bTiles[d] = solveArena_.Push(bt);
-            cp.bTilesN[d] = (int)bt.size();
+            cp.bN[d] = (int)bt.size();
+            cp.bGather[d] = solveArena_.Push(bg);
+            cp.bGatherN[d] = (int)bg.size();
         }
-        std::vector<int2> sc;
-        for (int t = 0; t < nn_; ++t)
-            for (int i0 = 0; i0 < cs.size[t]; i0 += kSolveRowTile) sc.push_back(make_int2(t, i0));
-        cp.sc = solveArena_.Push(sc);
-        cp.scN = (int)sc.size();
+        cp.pre = solveArena_.Push(pre);
+        cp.preN = (int)pre.size();
     }
+    partials_.Allocate((size_t)maxSlots * kSweepRows * kSweepCols * sizeof(cpx<R>));
+    counters_.Allocate((size_t)maxCounters * sizeof(int));
+    CUDA_CHECK(cudaMemsetAsync(counters_.p, 0, counters_.bytes, h_.stream_));
     solveArena_.Upload(h_.stream_);
     planK_ = k;
 }
@@ -527,27 +651,97 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     io.inMode = inMode;
     io.outAccumulate = outAcc;
     io.sp = h_.sp_;
-    const SolveFront<R>* fr = solveArena_.At<SolveFront<R>>(panelFronts_[p]);
-    const GemmOp<R>* fo = solveArena_.At<GemmOp<R>>(panelFwdOps_[p]);
-    const GemmOp<R>* bo = solveArena_.At<GemmOp<R>>(panelBwdOps_[p]);
+    const SweepFront<R>* fr = solveArena_.At<SweepFront<R>>(panelFronts_[p]);
+    SweepWork w;
+    w.partials = partials_.p;
+    w.counters = counters_.as<int>();
+    w.xnd = Xnd_.p;
     const int nd = (int)depthNodes_.size();
+    {
+        ProfScope ps(st, kProfGatherScatter);
+        LaunchSweepPregather<R>(fr, solveArena_.At<int2>(cp.pre), cp.preN, B, k, io, st);
+    }
     for (int d = nd - 1; d >= 0; --d) {
-        LaunchForwardGather<R>(fr, solveArena_.At<int2>(cp.fg[d]), cp.fgN[d], B, k, io, st);
-        LaunchGemm<R>(fo, solveArena_.At<GemmTile>(cp.fTiles[d]), cp.fTilesN[d], kGemmSkinny, st);
+        ProfScope ps(st, kProfSolveGemm, cp.fFlops[d], cp.fBytes[d]);
+        LaunchSweepForward<R>(fr, solveArena_.At<SweepTile>(cp.fTiles[d]), cp.fN[d], cp.fChunk[d], k, w, st);
     }
     for (int d = 0; d < nd; ++d) {
-        LaunchBackwardGather<R>(fr, solveArena_.At<int2>(cp.fg[d]), cp.fgN[d], k, st);
-        LaunchGemm<R>(bo, solveArena_.At<GemmTile>(cp.bTiles[d]), cp.bTilesN[d], kGemmSkinny, st);
+        {
+            ProfScope ps(st, kProfGatherScatter);
+            LaunchSweepBackwardGather<R>(fr, solveArena_.At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st);
+        }
+        ProfScope ps(st, kProfSolveGemm, cp.bFlops[d], cp.bBytes[d]);
+        LaunchSweepBackward<R>(fr, solveArena_.At<SweepTile>(cp.bTiles[d]), cp.bN[d], cp.bChunk[d], B, k, io, w,
+                               st);
     }
-    LaunchScatter<R>(fr, solveArena_.At<int2>(cp.sc), cp.scN, B, k, io, st);
 }
 
 template <typename R>
-void FactorStore<R>::Sweep(z64* B, int ldk, int k) {
+void FactorStore<R>::SweepEager(z64* B, int ldk, int k) {
     const int np = an_.geom.numPanels;
     for (int i = 0; i < np - 1; ++i) SolvePanel(B, ldk, k, i, i == 0 ? 0 : 1, 0);
     SolvePanel(B, ldk, k, np - 1, np - 1 == 0 ? 0 : 1, 0);
     for (int i = np - 2; i >= 0; --i) SolvePanel(B, ldk, k, i, 2, 1);
+}
+
+template <typename R>
+void FactorStore<R>::Sweep(z64* B, int ldk, int k, bool useGraph) {
+    Profiler* prof = CurrentProfiler();
+    const bool profiling = prof && prof->enabled;
+    if (!useGraph || profiling) {
+        ProfScope ps(h_.stream_, kProfSweep, SweepFlops(k), SweepBytes(k));
+        SweepEager(B, ldk, k);
+        return;
+    }
+    BuildSolvePlan(k);
+    for (const SweepGraph& g : graphs_)
+        if (g.B == B && g.ldk == ldk && g.k == k) {
+            CUDA_CHECK(cudaGraphLaunch(g.exec, h_.stream_));
+            return;
+        }
+    cudaGraph_t graph;
+    CUDA_CHECK(cudaStreamBeginCapture(h_.stream_, cudaStreamCaptureModeThreadLocal));
+    SweepEager(B, ldk, k);
+    CUDA_CHECK(cudaStreamEndCapture(h_.stream_, &graph));
+    SweepGraph g{B, ldk, k, nullptr};
+    CUDA_CHECK(cudaGraphInstantiate(&g.exec, graph, 0));
+    CUDA_CHECK(cudaGraphDestroy(graph));
+    graphs_.push_back(g);
+    CUDA_CHECK(cudaGraphLaunch(g.exec, h_.stream_));
+}
+
+// Algorithmic work of one sweep: every panel but the top one is solved twice.
+template <typename R>
+double FactorStore<R>::SweepFlops(int k) const {
+    const PanelGeometry& g = an_.geom;
+    double f = 0;
+    for (int p = 0; p < g.numPanels; ++p) {
+        const ClassStructure& cs = an_.cls[g.Class(p)];
+        double pf = 0;
+        for (size_t t = 0; t < cs.size.size(); ++t) {
+            const double s = cs.size[t], u = cs.usize[t];
+            pf += 8.0 * k * 2 * ((s + u) * s - s * (s - 1) / 2);
+        }
+        f += (p == g.numPanels - 1 ? 1 : 2) * pf;
+    }
+    return f;
+}
+
+template <typename R>
+double FactorStore<R>::SweepBytes(int k) const {
+    const PanelGeometry& g = an_.geom;
+    double b = 0;
+    for (int p = 0; p < g.numPanels; ++p) {
+        const ClassStructure& cs = an_.cls[g.Class(p)];
+        double pb = 0;
+        for (size_t t = 0; t < cs.size.size(); ++t) {
+            const double s = cs.size[t], u = cs.usize[t];
+            pb += 2.0 * sizeof(cpx<R>) * ((s + u) * s - s * (s - 1) / 2);
+        }
+        pb += 2.0 * 16.0 * k * g.Depth(p) * an_.disc.nx * an_.disc.ny;  // natural-order RHS in and out
+        b += (p == g.numPanels - 1 ? 1 : 2) * pb;
+    }
+    return b;
 }
 
 template class FactorStore<double>;
@@ -623,9 +817,11 @@ void Helmholtz::BuildTables() {
     sp_.s3 = dS3_.as<z64>(); sp_.is3 = sp_.s3 + (d.nz + 2);
     for (int c = 0; c < 3; ++c) {
         if (!an_.classUsed[c]) continue;
-        UploadVector(dNdToNat_[c], an_.cls[c].ndToNat, stream_);
-        UploadVector(dNbrRows_[c], an_.cls[c].nbrRows, stream_);
-        UploadVector(dRel_[c], an_.cls[c].rel, stream_);
+        const ClassStructure& cs = an_.cls[c];
+        UploadVector(dNdToNat_[c], cs.ndToNat, stream_);
+        UploadVector(dNbrRows_[c], cs.nbrRows, stream_);
+        UploadVector(dRel_[c], cs.rel, stream_);
+        UploadVector(dLower_[c], cs.lower, stream_);
         ap_.tabs.ndToNat[c] = dNdToNat_[c].as<int>();
         ap_.tabs.nbrRows[c] = dNbrRows_[c].as<int>();
     }
@@ -649,6 +845,7 @@ void Helmholtz::Initialize(const double* velocity, bool devicePtr, int panelSche
                                devicePtr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
     ap_.vel = dVel_.as<double>();
     precision_ = precision;
+    ProfilerBinding bind(&prof_);
     if (precision == 0) {
         f64_.reset(new FactorStore<double>(*this));
         f64_->Factor();
@@ -657,6 +854,7 @@ void Helmholtz::Initialize(const double* velocity, bool devicePtr, int panelSche
         f32_->Factor();
     }
     CUDA_CHECK(cudaStreamSynchronize(stream_));
+    if (prof_.enabled) prof_.Flush();
     initialized_ = true;
     setupSeconds_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -673,20 +871,34 @@ int64_t Helmholtz::factorBytes() const {
     return 0;
 }
 
-void Helmholtz::Precondition(z64* B, int k) {
+double Helmholtz::SweepFlops(int k) const {
+    if (f64_) return f64_->SweepFlops(k);
+    if (f32_) return f32_->SweepFlops(k);
+    return 0;
+}
+
+double Helmholtz::SweepBytes(int k) const {
+    if (f64_) return f64_->SweepBytes(k);
+    if (f32_) return f32_->SweepBytes(k);
+    return 0;
+}
+
+void Helmholtz::Precondition(z64* B, int k, bool useGraph) {
     constexpr int kBlock = 64;
     for (int r0 = 0; r0 < k; r0 += kBlock) {
         const int kb = std::min(kBlock, k - r0);
-        if (f64_) f64_->Sweep(B + r0, k, kb);
-        else f32_->Sweep(B + r0, k, kb);
+        if (f64_) f64_->Sweep(B + r0, k, kb, useGraph);
+        else f32_->Sweep(B + r0, k, kb, useGraph);
     }
 }
 
 void Helmholtz::PreconditionDevice(z64* B, int k) {
     if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
     CUDA_CHECK(cudaSetDevice(device_));
-    Precondition(B, k);
+    ProfilerBinding bind(&prof_);
+    Precondition(B, k, false);
     CUDA_CHECK(cudaStreamSynchronize(stream_));
+    if (prof_.enabled) prof_.Flush();
 }
 
 void Helmholtz::SolvePanelDevice(z64* B, int k, int panel) {
@@ -780,18 +992,22 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     auto fetch = [&](void* dst, const void* src, size_t bytes) {
         CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
     };
-    cudaEvent_t e0, e1;
-    CUDA_CHECK(cudaEventCreate(&e0));
-    CUDA_CHECK(cudaEventCreate(&e1));
-    auto timed = [&](double& acc, auto&& fn) {
-        CUDA_CHECK(cudaEventRecord(e0, st));
+    // Phase timing with events on the solve stream, resolved at the sync
+    // points GMRES needs anyway; per-kernel profiling nests inside when on.
+    ProfilerBinding bind(&prof_);
+    Profiler phases;
+    phases.enabled = true;
+    const double swFlops = SweepFlops(k), swBytes = SweepBytes(k);
+    auto timed = [&](int cat, double f, double by, auto&& fn) {
+        phases.Begin(st);
         fn();
-        CUDA_CHECK(cudaEventRecord(e1, st));
-        CUDA_CHECK(cudaEventSynchronize(e1));
-        float ms = 0;
-        CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        acc += ms * 1e-3;
+        phases.End(st, cat, f, by);
     };
+    auto precond = [&] {
+        timed(kProfSweep, swFlops, swBytes, [&] { Precondition(w, k, true); });
+        S.numPreconditions++;
+    };
+    const double mvFlops = 56.0 * nk, mvBytes = (double)N * (32.0 * k + 8);
 
     CUDA_CHECK(cudaMemcpyAsync(b, B, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
     CUDA_CHECK(cudaMemsetAsync(x, 0, nk * sizeof(z64), st));
@@ -809,8 +1025,7 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     double maxRel = 0;
     while (!converged) {
         CUDA_CHECK(cudaMemcpyAsync(x0, x, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
-        timed(S.precondSeconds, [&] { Precondition(w, k); });
-        S.numPreconditions++;
+        precond();
         norms(w, dNorm);
         fetch(beta.data(), dNorm, k * sizeof(double));
         CUDA_CHECK(cudaStreamSynchronize(st));
@@ -819,10 +1034,10 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
         std::fill(z.begin(), z.end(), Cd(0));
         for (int r = 0; r < k; ++r) z[(size_t)r * (m + 1)] = beta[r];
         for (int j = 0; j < m; ++j) {
-            timed(S.matvecSeconds, [&] { LaunchHelmholtzApply(V + (size_t)j * nk, w, nullptr, vel, sp_, k, st); });
-            timed(S.precondSeconds, [&] { Precondition(w, k); });
-            S.numPreconditions++;
-            const auto ta = std::chrono::steady_clock::now();
+            timed(kProfStencil, mvFlops, mvBytes,
+                  [&] { LaunchHelmholtzApply(V + (size_t)j * nk, w, nullptr, vel, sp_, k, st); });
+            precond();
+            phases.Begin(st);
             for (int i = 0; i <= j; ++i) {
                 LaunchMgsStep(w, i > 0 ? V + (size_t)(i - 1) * nk : nullptr, i > 0 ? dH + (size_t)(i - 1) * k : nullptr,
                               V + (size_t)i * nk, N, k, dPartial_.as<z64>(), st);
@@ -830,6 +1045,7 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
             }
             LaunchAxpyColumns(w, V + (size_t)j * nk, dH + (size_t)j * k, N, k, st);
             norms(w, dDelta);
+            phases.End(st, kProfVector, 8.0 * 2 * (j + 1) * nk, 16.0 * (3 * (j + 1) + 2) * nk);
             hcol.resize((size_t)(j + 1) * k);
             fetch(hcol.data(), dH, (size_t)(j + 1) * k * sizeof(z64));
             fetch(delta.data(), dDelta, k * sizeof(double));
@@ -844,10 +1060,9 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
                 S.iterations = it;
                 S.finalMaxRelResid = maxRel;
                 S.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
                 return;
             }
+            phases.Begin(st);
             if (j + 1 != m) LaunchScaleColumns(w, dDelta, V + (size_t)(j + 1) * nk, N, k, st);
             for (int r = 0; r < k; ++r) {
                 Cd* Hr = &H[(size_t)r * m * m];
@@ -880,11 +1095,12 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
             }
             CUDA_CHECK(cudaMemcpyAsync(dY, y.data(), (size_t)(j + 1) * k * sizeof(z64), cudaMemcpyHostToDevice, st));
             LaunchCombine(x0, V, nk, dY, j + 1, x, N, k, st);
-            timed(S.matvecSeconds, [&] { LaunchHelmholtzApply(x, w, b, vel, sp_, k, st); });
+            phases.End(st, kProfVector, 8.0 * (j + 1) * nk, 16.0 * (j + 3) * nk);
+            timed(kProfStencil, mvFlops, mvBytes + 16.0 * nk, [&] { LaunchHelmholtzApply(x, w, b, vel, sp_, k, st); });
             norms(w, dNorm);
             fetch(resid.data(), dNorm, k * sizeof(double));
             CUDA_CHECK(cudaStreamSynchronize(st));
-            S.arnoldiSeconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count();
+            phases.Flush();
             if (AnyNaN(resid)) throw PspError(kRuntimeError, "resid norm list has NaN");
             maxRel = 0;
             for (int r = 0; r < k; ++r) maxRel = std::max(maxRel, resid[r] / origResid[r]);
@@ -900,8 +1116,11 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     }
     CUDA_CHECK(cudaMemcpyAsync(B, x, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));
     CUDA_CHECK(cudaStreamSynchronize(st));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    phases.Flush();
+    if (prof_.enabled) prof_.Flush();
+    S.precondSeconds = phases.totals[kProfSweep].ms * 1e-3;
+    S.matvecSeconds = phases.totals[kProfStencil].ms * 1e-3;
+    S.arnoldiSeconds = phases.totals[kProfVector].ms * 1e-3;
     S.iterations = it;
     S.converged = converged ? 1 : 0;
     S.finalMaxRelResid = maxRel;

@@ -8,6 +8,7 @@
 
 #include "analysis.hpp"
 #include "kernels.cuh"
+#include "profiler.hpp"
 
 namespace psp_b200 {
 
@@ -55,10 +56,15 @@ struct SolveStats {
     std::vector<double> history;
 };
 
-struct PanelPlan;  // per class solve task lists
-
 template <typename R>
 class FactorStore;
+
+// Makes `p` the profiler of launches issued by this thread while in scope.
+struct ProfilerBinding {
+    Profiler* prev;
+    explicit ProfilerBinding(Profiler* p) : prev(CurrentProfiler()) { CurrentProfiler() = p; }
+    ~ProfilerBinding() { CurrentProfiler() = prev; }
+};
 
 class Helmholtz {
 public:
@@ -86,13 +92,17 @@ public:
     double setupSeconds() const { return setupSeconds_; }
     int64_t factorBytes() const;
     void SetMaxIterations(int n) { maxIterations_ = n; }
+    Profiler& profiler() { return prof_; }
+    // Sweep algorithmic flops/bytes for k right-hand sides (0 before Initialize).
+    double SweepFlops(int k) const;
+    double SweepBytes(int k) const;
 
     // Device tables shared with the factor stores.
     StencilParams sp_{};
     AssemblyParams ap_{};
     DeviceBuffer dS1_, dS2_, dS3_, dS3a_;   // values and reciprocals back to back
     DeviceBuffer dVel_;
-    DeviceBuffer dNdToNat_[3], dNbrRows_[3], dRel_[3];
+    DeviceBuffer dNdToNat_[3], dNbrRows_[3], dRel_[3], dLower_[3];
     std::vector<int> s3aOff_;                // per panel
     Analysis an_;
     double damping_;
@@ -101,9 +111,10 @@ public:
 
 private:
     void BuildTables();
-    void Precondition(z64* B, int k);
+    void Precondition(z64* B, int k, bool useGraph);
     void EnsureWorkspace(int k, int m);
 
+    Profiler prof_;
     bool initialized_ = false;
     int precision_ = 0;
     int maxIterations_ = 0;
