@@ -161,7 +161,6 @@ private:
     std::vector<SweepGraph> graphs_;
     void SweepEager(z64* B, int ldk, int k);
     void FactorGroup(int p0, int p1, FactorFront<R>* hostFronts, std::vector<FactorFront<R>>& all);
-    void BuildSolvePlan(int k);
 
     Helmholtz& h_;
     const Analysis& an_;
@@ -170,18 +169,24 @@ private:
     std::vector<int64_t> gOff_, dOff_;
     std::vector<std::vector<int>> depthNodes_;
     DeviceBuffer status_;
-    // solve plan for one RHS block width
-    int planK_ = -1;
-    DeviceBuffer Rb_, Y_, Z_, Xnd_, partials_, counters_;
-    TaskArena solveArena_;
     struct ClassPlan {
         size_t pre = 0;
         int preN = 0;
         std::vector<size_t> fTiles, bTiles, bGather;
         std::vector<int> fN, bN, bGatherN, fChunk, bChunk;
         std::vector<double> fFlops, fBytes, bFlops, bBytes;
-    } cplan_[3];
-    std::vector<size_t> panelFronts_;
+    };
+    // Task lists and work vectors of the panel solves for one RHS block width.
+    // Plans live as long as the factors: captured sweep graphs point into them.
+    struct SolvePlan {
+        int k = 0;
+        DeviceBuffer Rb, Y, Z, Xnd, partials, counters;
+        TaskArena arena;
+        ClassPlan cplan[3];
+        std::vector<size_t> panelFronts;
+    };
+    std::vector<std::unique_ptr<SolvePlan>> plans_;
+    SolvePlan& Plan(int k);
 };
 
 template <typename R>
@@ -488,8 +493,12 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
 }
 
 template <typename R>
-void FactorStore<R>::BuildSolvePlan(int k) {
-    if (planK_ == k) return;
+typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
+    for (auto& pl : plans_)
+        if (pl->k == k) return *pl;
+    plans_.emplace_back(new SolvePlan);
+    SolvePlan& P = *plans_.back();
+    P.k = k;
     const PanelGeometry& g = an_.geom;
     const XYTree& tree = an_.tree;
     const int np = g.numPanels;
@@ -512,12 +521,12 @@ void FactorStore<R>::BuildSolvePlan(int k) {
         maxR = std::max(maxR, tr); maxY = std::max(maxY, ty); maxZ = std::max(maxZ, tz);
         maxSub = std::max(maxSub, cs.nSub);
     }
-    Rb_.Allocate(maxR * sizeof(cpx<R>));
-    Y_.Allocate(maxY * sizeof(cpx<R>));
-    Z_.Allocate(maxZ * sizeof(cpx<R>));
-    Xnd_.Allocate((size_t)maxSub * k * sizeof(cpx<R>));
-    solveArena_.host.clear();
-    panelFronts_.assign(np, 0);
+    P.Rb.Allocate(maxR * sizeof(cpx<R>));
+    P.Y.Allocate(maxY * sizeof(cpx<R>));
+    P.Z.Allocate(maxZ * sizeof(cpx<R>));
+    P.Xnd.Allocate((size_t)maxSub * k * sizeof(cpx<R>));
+    P.arena.host.clear();
+    P.panelFronts.assign(np, 0);
     for (int p = 0; p < np; ++p) {
         const int c = g.Class(p);
         const ClassStructure& cs = an_.cls[c];
@@ -527,10 +536,10 @@ void FactorStore<R>::BuildSolvePlan(int k) {
             const XYNode& node = tree.nodes[t];
             f.G = G_.as<cpx<R>>() + gOff_[(size_t)p * nn_ + t];
             f.D = D_.as<cpx<R>>() + dOff_[(size_t)p * nn_ + t];
-            f.Rb = Rb_.as<cpx<R>>() + rOff[c][t];
-            f.parentRb = node.parent >= 0 ? Rb_.as<cpx<R>>() + rOff[c][node.parent] : nullptr;
-            f.Y = Y_.as<cpx<R>>() + yOff[c][t];
-            f.Z = Z_.as<cpx<R>>() + zOff[c][t];
+            f.Rb = P.Rb.template as<cpx<R>>() + rOff[c][t];
+            f.parentRb = node.parent >= 0 ? P.Rb.template as<cpx<R>>() + rOff[c][node.parent] : nullptr;
+            f.Y = P.Y.template as<cpx<R>>() + yOff[c][t];
+            f.Z = P.Z.template as<cpx<R>>() + zOff[c][t];
             f.lower = h_.dLower_[c].as<int>() + cs.lowerOff[t];
             f.rel = h_.dRel_[c].as<int>() + cs.lowerOff[t];
             f.s = cs.size[t];
@@ -538,7 +547,7 @@ void FactorStore<R>::BuildSolvePlan(int k) {
             f.ndOff = cs.off[t];
             f.childSlot = (node.parent >= 0 && tree.nodes[node.parent].child[1] == t) ? 1 : 0;
         }
-        panelFronts_[p] = solveArena_.Push(fr);
+        P.panelFronts[p] = P.arena.Push(fr);
     }
     // Tiles of one depth and direction.  The K-chunk shrinks until the launch
     // has a few CTAs per SM; rows of a tile share one K range (inv(L11) is
@@ -598,7 +607,7 @@ void FactorStore<R>::BuildSolvePlan(int k) {
     for (int c = 0; c < 3; ++c) {
         if (!an_.classUsed[c]) continue;
         const ClassStructure& cs = an_.cls[c];
-        ClassPlan& cp = cplan_[c];
+        ClassPlan& cp = P.cplan[c];
         cp.fTiles.assign(nd, 0); cp.bTiles.assign(nd, 0); cp.bGather.assign(nd, 0);
         cp.fN.assign(nd, 0); cp.bN.assign(nd, 0); cp.bGatherN.assign(nd, 0);
         cp.fChunk.assign(nd, 0); cp.bChunk.assign(nd, 0);
@@ -614,29 +623,29 @@ void FactorStore<R>::BuildSolvePlan(int k) {
                     bg.push_back(make_int2(t, i0));
                     pre.push_back(make_int2(t, i0));
                 }
-            cp.fTiles[d] = solveArena_.Push(ft);
+            cp.fTiles[d] = P.arena.Push(ft);
             cp.fN[d] = (int)ft.size();
-            cp.bTiles[d] = solveArena_.Push(bt);
+            cp.bTiles[d] = P.arena.Push(bt);
             cp.bN[d] = (int)bt.size();
-            cp.bGather[d] = solveArena_.Push(bg);
+            cp.bGather[d] = P.arena.Push(bg);
             cp.bGatherN[d] = (int)bg.size();
         }
-        cp.pre = solveArena_.Push(pre);
+        cp.pre = P.arena.Push(pre);
         cp.preN = (int)pre.size();
     }
-    partials_.Allocate((size_t)maxSlots * kSweepRows * kSweepCols * sizeof(cpx<R>));
-    counters_.Allocate((size_t)maxCounters * sizeof(int));
-    CUDA_CHECK(cudaMemsetAsync(counters_.p, 0, counters_.bytes, h_.stream_));
-    solveArena_.Upload(h_.stream_);
-    planK_ = k;
+    P.partials.Allocate((size_t)maxSlots * kSweepRows * kSweepCols * sizeof(cpx<R>));
+    P.counters.Allocate((size_t)maxCounters * sizeof(int));
+    CUDA_CHECK(cudaMemsetAsync(P.counters.p, 0, P.counters.bytes, h_.stream_));
+    P.arena.Upload(h_.stream_);
+    return P;
 }
 
 template <typename R>
 void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc) {
-    BuildSolvePlan(k);
+    SolvePlan& P = Plan(k);
     const PanelGeometry& g = an_.geom;
     const int c = g.Class(p);
-    const ClassPlan& cp = cplan_[c];
+    const ClassPlan& cp = P.cplan[c];
     cudaStream_t st = h_.stream_;
     PanelIO io;
     io.ndToNat = h_.dNdToNat_[c].as<int>();
@@ -651,27 +660,27 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     io.inMode = inMode;
     io.outAccumulate = outAcc;
     io.sp = h_.sp_;
-    const SweepFront<R>* fr = solveArena_.At<SweepFront<R>>(panelFronts_[p]);
+    const SweepFront<R>* fr = P.arena.template At<SweepFront<R>>(P.panelFronts[p]);
     SweepWork w;
-    w.partials = partials_.p;
-    w.counters = counters_.as<int>();
-    w.xnd = Xnd_.p;
+    w.partials = P.partials.p;
+    w.counters = P.counters.template as<int>();
+    w.xnd = P.Xnd.p;
     const int nd = (int)depthNodes_.size();
     {
         ProfScope ps(st, kProfGatherScatter);
-        LaunchSweepPregather<R>(fr, solveArena_.At<int2>(cp.pre), cp.preN, B, k, io, st);
+        LaunchSweepPregather<R>(fr, P.arena.template At<int2>(cp.pre), cp.preN, B, k, io, st);
     }
     for (int d = nd - 1; d >= 0; --d) {
         ProfScope ps(st, kProfSolveGemm, cp.fFlops[d], cp.fBytes[d]);
-        LaunchSweepForward<R>(fr, solveArena_.At<SweepTile>(cp.fTiles[d]), cp.fN[d], cp.fChunk[d], k, w, st);
+        LaunchSweepForward<R>(fr, P.arena.template At<SweepTile>(cp.fTiles[d]), cp.fN[d], cp.fChunk[d], k, w, st);
     }
     for (int d = 0; d < nd; ++d) {
         {
             ProfScope ps(st, kProfGatherScatter);
-            LaunchSweepBackwardGather<R>(fr, solveArena_.At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st);
+            LaunchSweepBackwardGather<R>(fr, P.arena.template At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st);
         }
         ProfScope ps(st, kProfSolveGemm, cp.bFlops[d], cp.bBytes[d]);
-        LaunchSweepBackward<R>(fr, solveArena_.At<SweepTile>(cp.bTiles[d]), cp.bN[d], cp.bChunk[d], B, k, io, w,
+        LaunchSweepBackward<R>(fr, P.arena.template At<SweepTile>(cp.bTiles[d]), cp.bN[d], cp.bChunk[d], B, k, io, w,
                                st);
     }
 }
@@ -693,7 +702,7 @@ void FactorStore<R>::Sweep(z64* B, int ldk, int k, bool useGraph) {
         SweepEager(B, ldk, k);
         return;
     }
-    BuildSolvePlan(k);
+    Plan(k);  // built outside the capture: it allocates and uploads
     for (const SweepGraph& g : graphs_)
         if (g.B == B && g.ldk == ldk && g.k == k) {
             CUDA_CHECK(cudaGraphLaunch(g.exec, h_.stream_));
@@ -883,10 +892,18 @@ double Helmholtz::SweepBytes(int k) const {
     return 0;
 }
 
+// Right-hand sides go through the sweep in blocks of equal width (at most
+// kRhsBlock), so one solve plan serves every block.
+constexpr int kRhsBlock = 64;
+static int RhsBlockWidth(int k) {
+    const int nb = (k + kRhsBlock - 1) / kRhsBlock;
+    return (k + nb - 1) / nb;
+}
+
 void Helmholtz::Precondition(z64* B, int k, bool useGraph) {
-    constexpr int kBlock = 64;
-    for (int r0 = 0; r0 < k; r0 += kBlock) {
-        const int kb = std::min(kBlock, k - r0);
+    const int w = RhsBlockWidth(k);
+    for (int r0 = 0; r0 < k; r0 += w) {
+        const int kb = std::min(w, k - r0);
         if (f64_) f64_->Sweep(B + r0, k, kb, useGraph);
         else f32_->Sweep(B + r0, k, kb, useGraph);
     }
@@ -905,9 +922,9 @@ void Helmholtz::SolvePanelDevice(z64* B, int k, int panel) {
     if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
     if (panel < 0 || panel >= an_.geom.numPanels) throw PspError(kLogicError, "panel index out of range");
     CUDA_CHECK(cudaSetDevice(device_));
-    constexpr int kBlock = 64;
-    for (int r0 = 0; r0 < k; r0 += kBlock) {
-        const int kb = std::min(kBlock, k - r0);
+    const int w = RhsBlockWidth(k);
+    for (int r0 = 0; r0 < k; r0 += w) {
+        const int kb = std::min(w, k - r0);
         if (f64_) f64_->SolvePanel(B + r0, k, kb, panel, 0, 0);
         else f32_->SolvePanel(B + r0, k, kb, panel, 0, 0);
     }
