@@ -133,6 +133,12 @@ class Oracle:
         if lib().oracle_initialize(self._h, _ptr(v)):
             raise RuntimeError(lib().oracle_last_error().decode())
 
+    def form_operator(self, velocity):
+        """Forms the global operator only (no panel factorization)."""
+        v = np.ascontiguousarray(velocity, dtype=np.float64)
+        lib().oracle_form_operator.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+        lib().oracle_form_operator(self._h, _ptr(v))
+
     def global_operator_natural(self):
         """The global operator as a scipy CSR matrix in natural ordering."""
         import scipy.sparse as sp

@@ -878,9 +878,17 @@ static void Push(const Solver& S, C* grid, int k, const std::vector<C>& B) {
         for (int r = 0; r < k; ++r) grid[(size_t)S.ndToNat[i] * k + r] = B[i + (size_t)r * S.N];
 }
 
+// Forms the global operator only (FormGlobalRow for every row).
+int oracle_form_operator(void* h, const double* velocity) {
+    Solver& S = *(Solver*)h;
+    FormGlobalOperator(S, velocity);
+    return 0;
+}
+
 // B := A B on a natural-order interleaved grid (complex as 2 doubles).
 int oracle_multiply(void* h, double* grid, int k) {
     Solver& S = *(Solver*)h;
+    if (S.rowPtr.empty()) { g_err = "global operator not formed"; return 1; }
     std::vector<C> B;
     Pull(S, (C*)grid, k, B);
     Multiply(S, B.data(), k);

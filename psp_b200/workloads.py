@@ -137,4 +137,6 @@ def small_case(interior=(12, 13, 14), pml=5, freq=2.0, k=3, seed=7, top_pml=True
 CONFIGS = {
     "plain_bump_50": plain_bump,
     "smooth_anomalies_116": smooth_anomalies,
+    # profiling-sized member of the same family (factors ~0.5 GB, above L2)
+    "smooth_anomalies_56": lambda: smooth_anomalies(interior=(40, 40, 40), pml=8, freq=4.0, k=16),
 }
