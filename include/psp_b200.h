@@ -106,6 +106,19 @@ int psp_cu_precondition(psp_cu_handle* h, double* B, int k);
 int psp_cu_multiply_device(psp_cu_handle* h, double* d_B, int k);
 int psp_cu_precondition_device(psp_cu_handle* h, double* d_B, int k);
 
+/* B := A B on a device grid without allocating any device memory.  No
+ * counterpart in the reference: it exists for callers that cannot allocate
+ * while they call -- code running inside its own CUDA stream capture, where an
+ * allocation breaks the capture, and services that reserve all device memory
+ * up front.  psp_cu_multiply_device allocates its nx*ny*nz*k temporary on
+ * every call; this variant uses a 16 MiB file-scope device array instead, so
+ * nx*ny*nz*k must not exceed 1048576 (PSP_CU_LOGIC_ERROR otherwise).  The
+ * first call on a device looks up that array's device address; make it before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be ordered by the caller.  Requires an initialized
+ * handle. */
+int psp_cu_multiply_device_noalloc(psp_cu_handle* h, double* d_B, int k);
+
 /* B := T_p B on panel p only (SolvePanel, solve.hpp:736-882); host grid. */
 int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel);
 

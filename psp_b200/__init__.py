@@ -71,6 +71,7 @@ C_ABI_SYMBOLS = [
     "psp_cu_multiply_device", "psp_cu_precondition_device", "psp_cu_solve_panel", "psp_cu_set_max_iterations",
     "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class", "psp_cu_get_stream",
     "psp_cu_set_profiling", "psp_cu_profile_reset", "psp_cu_profile_get", "psp_cu_sweep_cost",
+    "psp_cu_multiply_device_noalloc",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -113,6 +114,7 @@ def lib():
         L.psp_cu_profile_reset.argtypes = [vp]
         L.psp_cu_profile_get.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp]
         L.psp_cu_sweep_cost.argtypes = [vp, ctypes.c_int, dp, dp]
+        L.psp_cu_multiply_device_noalloc.argtypes = [vp, vp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -367,6 +369,13 @@ class DistHelmholtz:
 
     def multiply_device(self, B):
         _check(lib().psp_cu_multiply_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+
+    def multiply_device_noalloc(self, B):
+        """B := A B in place on a CUDA tensor without any device allocation
+        (for callers inside their own stream capture, or with a fixed memory
+        reservation); nx*ny*nz*k must not exceed 1048576, and calls that
+        overlap on the GPU race on the shared scratch array."""
+        _check(lib().psp_cu_multiply_device_noalloc(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
 
     def precondition_device(self, B):
         _check(lib().psp_cu_precondition_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))

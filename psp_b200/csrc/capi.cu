@@ -5,14 +5,11 @@
 #include <string>
 
 #include "../../include/psp_b200.h"
+#include "handle.hpp"
 #include "solver.hpp"
 
 using psp_b200::Helmholtz;
 using psp_b200::PspError;
-
-struct psp_cu_handle {
-    Helmholtz* solver;
-};
 
 namespace {
 
@@ -75,6 +72,10 @@ void OnDeviceCopy(Helmholtz* s, double* B, int k, F&& fn) {
 }
 
 }  // namespace
+
+namespace psp_b200 {
+void SetLastError(const std::string& msg) { g_lastError = msg; }
+}  // namespace psp_b200
 
 extern "C" {
 
