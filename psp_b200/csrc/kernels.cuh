@@ -135,13 +135,17 @@ constexpr int kSweepThreads = kSweepRows * kSweepSlices;
 constexpr int kSweepCols = 16;
 constexpr size_t kSweepSmemBytes = 32 * 1024;  // staged right-hand-side chunk
 
-// Device scratch of the sweep: split-K partials (kSweepRows*kSweepCols
-// complex entries per slot), arrival counters (zero between launches) and the
-// panel's ND-ordered solution vector [ND index][k].
+constexpr int kTcRows = 128;       // rows per CTA of the tensor-core sweep kernels (UMMA M)
+
+// Device scratch of the sweep: split-K partials (rows-per-tile * kSweepCols
+// complex entries per slot), arrival counters (zero between launches), the
+// panel's ND-ordered solution vector [ND index][k] and a status word (bit 2:
+// a tensor-core pipeline wait timed out).
 struct SweepWork {
     void* partials;
     int* counters;
     void* xnd;
+    int* status;
 };
 
 struct PanelIO {
@@ -175,6 +179,14 @@ void LaunchSweepBackwardGather(const SweepFront<R>* fr, const int2* tasks, int n
 template <typename R>
 void LaunchSweepBackward(const SweepFront<R>* fr, const SweepTile* tiles, int n, int maxChunk, z64* B, int k,
                          const PanelIO& io, const SweepWork& w, cudaStream_t st);
+
+// Tensor-core (tcgen05, split TF32) forms for complex-single factors
+// (sweep_tc.cu); tiles of kTcRows rows, any K-chunk length.
+void PrepareSweepTcKernels();
+void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, const SweepWork& w,
+                          cudaStream_t st);
+void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k,
+                           const PanelIO& io, const SweepWork& w, cudaStream_t st);
 
 // ------------------------------------------------------------------ GMRES vectors
 

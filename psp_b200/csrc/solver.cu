@@ -5,7 +5,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 #include "solver.hpp"
 
@@ -132,7 +134,14 @@ GemmOp<R> MakeOp(const cpx<R>* A, int64_t lda, int transA, const cpx<R>* B, int6
 template <typename R>
 class FactorStore {
 public:
-    explicit FactorStore(Helmholtz& h) : h_(h), an_(h.an_) { PrepareSweepKernels<R>(); }
+    explicit FactorStore(Helmholtz& h) : h_(h), an_(h.an_) {
+        PrepareSweepKernels<R>();
+        // Complex-single factors use the tensor-core sweep unless the
+        // environment asks for the CUDA-core kernels (for comparisons).
+        const char* env = std::getenv("PSP_B200_SWEEP_CUDA_CORES");
+        tc_ = std::is_same<R, float>::value && !(env && env[0] == '1');
+        if (tc_) PrepareSweepTcKernels();
+    }
     ~FactorStore() {
         for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
     }
@@ -142,6 +151,14 @@ public:
     // `useGraph` and profiling is off.
     void Sweep(z64* B, int ldk, int k, bool useGraph);
     int64_t Bytes() const { return (int64_t)(G_.bytes + D_.bytes); }
+    // Device status word: bit 1 zero/non-finite pivot, bit 2 a tensor-core
+    // pipeline wait timed out.  Synchronizes the stream.
+    int ReadStatus() {
+        int st = 0;
+        CUDA_CHECK(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, h_.stream_));
+        CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
+        return st;
+    }
     double SweepFlops(int k) const;
     double SweepBytes(int k) const;
 
@@ -187,6 +204,8 @@ private:
     };
     std::vector<std::unique_ptr<SolvePlan>> plans_;
     SolvePlan& Plan(int k);
+    bool tc_ = false;  // tensor-core sweep kernels (complex single only)
+    int TileRows() const { return tc_ ? kTcRows : kSweepRows; }
 };
 
 template <typename R>
@@ -553,7 +572,10 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // has a few CTAs per SM; rows of a tile share one K range (inv(L11) is
     // triangular, so the forward range stops at the tile's last row and the
     // backward range starts at its first).
-    const int maxChunk = SweepMaxChunk<R>();
+    // Tensor-core CTAs stream their chunk in 16-column stages, one stage per
+    // load latency: short chunks keep CTAs uniform and launches tail-free.
+    const int maxChunk = tc_ ? 128 : SweepMaxChunk<R>();
+    const int tileRows = TileRows();
     int64_t maxSlots = 1, maxCounters = 1;
     auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepTile>& tiles, int& chunk,
                          double& flops, double& bytes) {
@@ -563,9 +585,9 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
                 const int s = cs.size[t], u = cs.usize[t];
                 const int M = fwd ? s + u : s, K = fwd ? s : s + u;
                 for (int col0 = 0; col0 < k; col0 += kSweepCols)
-                    for (int row0 = 0; row0 < M; row0 += kSweepRows) {
+                    for (int row0 = 0; row0 < M; row0 += tileRows) {
                         const int kb = fwd ? 0 : row0;
-                        const int ke = fwd ? std::min(K, row0 + kSweepRows) : K;
+                        const int ke = fwd ? std::min(K, row0 + tileRows) : K;
                         const int ns = std::max(1, (int)CeilDiv(ke - kb, kc));
                         for (int sp = 0; sp < ns; ++sp) {
                             if (emit) {
@@ -633,7 +655,7 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
         cp.pre = P.arena.Push(pre);
         cp.preN = (int)pre.size();
     }
-    P.partials.Allocate((size_t)maxSlots * kSweepRows * kSweepCols * sizeof(cpx<R>));
+    P.partials.Allocate((size_t)maxSlots * tileRows * kSweepCols * sizeof(cpx<R>));
     P.counters.Allocate((size_t)maxCounters * sizeof(int));
     CUDA_CHECK(cudaMemsetAsync(P.counters.p, 0, P.counters.bytes, h_.stream_));
     P.arena.Upload(h_.stream_);
@@ -665,6 +687,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     w.partials = P.partials.p;
     w.counters = P.counters.template as<int>();
     w.xnd = P.Xnd.p;
+    w.status = status_.template as<int>();
     const int nd = (int)depthNodes_.size();
     {
         ProfScope ps(st, kProfGatherScatter);
@@ -672,7 +695,14 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     }
     for (int d = nd - 1; d >= 0; --d) {
         ProfScope ps(st, kProfSolveGemm, cp.fFlops[d], cp.fBytes[d]);
-        LaunchSweepForward<R>(fr, P.arena.template At<SweepTile>(cp.fTiles[d]), cp.fN[d], cp.fChunk[d], k, w, st);
+        const SweepTile* tl = P.arena.template At<SweepTile>(cp.fTiles[d]);
+        if constexpr (std::is_same<R, float>::value) {
+            if (tc_) {
+                LaunchSweepForwardTc(fr, tl, cp.fN[d], k, w, st);
+                continue;
+            }
+        }
+        LaunchSweepForward<R>(fr, tl, cp.fN[d], cp.fChunk[d], k, w, st);
     }
     for (int d = 0; d < nd; ++d) {
         {
@@ -680,8 +710,14 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
             LaunchSweepBackwardGather<R>(fr, P.arena.template At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st);
         }
         ProfScope ps(st, kProfSolveGemm, cp.bFlops[d], cp.bBytes[d]);
-        LaunchSweepBackward<R>(fr, P.arena.template At<SweepTile>(cp.bTiles[d]), cp.bN[d], cp.bChunk[d], B, k, io, w,
-                               st);
+        const SweepTile* tl = P.arena.template At<SweepTile>(cp.bTiles[d]);
+        if constexpr (std::is_same<R, float>::value) {
+            if (tc_) {
+                LaunchSweepBackwardTc(fr, tl, cp.bN[d], B, k, io, w, st);
+                continue;
+            }
+        }
+        LaunchSweepBackward<R>(fr, tl, cp.bN[d], cp.bChunk[d], B, k, io, w, st);
     }
 }
 
@@ -909,6 +945,11 @@ void Helmholtz::Precondition(z64* B, int k, bool useGraph) {
     }
 }
 
+void Helmholtz::CheckSweepStatus() {
+    const int st = f64_ ? f64_->ReadStatus() : (f32_ ? f32_->ReadStatus() : 0);
+    if (st & 2) throw PspError(kRuntimeError, "a tensor-core pipeline wait timed out in the sweep");
+}
+
 void Helmholtz::PreconditionDevice(z64* B, int k) {
     if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
     CUDA_CHECK(cudaSetDevice(device_));
@@ -916,6 +957,7 @@ void Helmholtz::PreconditionDevice(z64* B, int k) {
     Precondition(B, k, false);
     CUDA_CHECK(cudaStreamSynchronize(stream_));
     if (prof_.enabled) prof_.Flush();
+    CheckSweepStatus();
 }
 
 void Helmholtz::SolvePanelDevice(z64* B, int k, int panel) {
@@ -1135,6 +1177,7 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     CUDA_CHECK(cudaStreamSynchronize(st));
     phases.Flush();
     if (prof_.enabled) prof_.Flush();
+    CheckSweepStatus();
     S.precondSeconds = phases.totals[kProfSweep].ms * 1e-3;
     S.matvecSeconds = phases.totals[kProfStencil].ms * 1e-3;
     S.arnoldiSeconds = phases.totals[kProfVector].ms * 1e-3;

@@ -113,6 +113,7 @@ private:
     void BuildTables();
     void Precondition(z64* B, int k, bool useGraph);
     void EnsureWorkspace(int k, int m);
+    void CheckSweepStatus();
 
     Profiler prof_;
     bool initialized_ = false;

@@ -1,0 +1,134 @@
+// Minimal sm_100a tensor-core toolkit: tcgen05 MMA with operands in shared
+// memory and the accumulator in tensor memory (TMEM), completion through
+// mbarriers.  Layout and descriptor encodings follow the sm100 UMMA
+// definitions (SWIZZLE_NONE, K-major canonical layout):
+//   a K-major operand tile of R rows x K tf32 values is stored as 8-row x
+//   16-byte "core matrices" (rows 16 B apart); the K-chunks of one 8-row
+//   group are kChunkBytes apart (the descriptor's leading byte offset) and
+//   consecutive 8-row groups are sbo bytes apart (its stride byte offset).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace psp_b200 {
+namespace umma {
+
+constexpr uint32_t kChunkBytes = 128;  // one core matrix: 8 rows x 16 bytes
+
+// Byte offset of element (row, k) of a K-major tile whose 8-row groups are
+// `sbo` bytes apart.
+__device__ __forceinline__ uint32_t KMajorOffset(int row, int k, uint32_t sbo) {
+    return (uint32_t)(row >> 3) * sbo + (uint32_t)(k >> 2) * kChunkBytes + (uint32_t)(row & 7) * 16u +
+           (uint32_t)(k & 3) * 4u;
+}
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start address, leading byte offset (between
+// the two 16-byte K-chunks an MMA consumes), stride byte offset (between
+// 8-row groups), version 1, no swizzle.
+__device__ __forceinline__ uint64_t SmemDesc(uint32_t smemAddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smemAddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm100
+    return d;
+}
+
+// Instruction descriptor: D f32, A and B tf32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t InstrDescTf32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void MmaTf32(uint32_t tmemD, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmemD), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// Arrive on `mbar` once every tcgen05 operation issued so far by this thread
+// has completed.
+__device__ __forceinline__ void CommitTo(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(SmemAddr(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void FenceBeforeSync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void FenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Generic-proxy shared-memory writes become visible to the tensor core.
+__device__ __forceinline__ void FenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void MbarInit(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(mbar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void FenceMbarInit() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ bool MbarTryWait(uint64_t* mbar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(SmemAddr(mbar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for `phase` of `mbar`; false (and *status set) on timeout.
+__device__ __forceinline__ bool MbarWaitBounded(uint64_t* mbar, uint32_t phase, int* status) {
+    constexpr uint32_t kMaxTries = 1u << 22;
+    for (uint32_t i = 0; i < kMaxTries; ++i)
+        if (MbarTryWait(mbar, phase)) return true;
+    if (status) atomicOr(status, 2);
+    return false;
+}
+
+// TMEM allocation by one full warp; the column address lands in *slot.
+__device__ __forceinline__ void TmemAlloc(uint32_t* slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void TmemDealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 32 consecutive f32 columns of this thread's TMEM lane (lane = row of D).
+__device__ __forceinline__ void TmemLoad32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Split x into a tf32 head and a tf32 tail: x ~= hi + lo to ~2^-22 relative.
+__device__ __forceinline__ void SplitTf32(float x, float& hi, float& lo) {
+    uint32_t h;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+    hi = __uint_as_float(h);
+    uint32_t l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
+    lo = __uint_as_float(l);
+}
+
+}  // namespace umma
+}  // namespace psp_b200
