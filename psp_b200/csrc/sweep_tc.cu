@@ -8,14 +8,28 @@
 // B becomes the 2x2 real block [[re b, im b], [-im b, re b]] of a 2K x 32
 // real matrix, so the 32 real accumulator columns are C's interleaved
 // (re, im) pairs.  Each operand is split into tf32 head and tail
-// (x = hi + lo) and the products hi*hi + hi*lo + lo*hi are accumulated in
-// FP32 in tensor memory: about FP32 accuracy from TF32 inputs.
+// (x = hi + lo) and hi*hi + hi*lo + lo*hi is accumulated in FP32 in tensor
+// memory (about FP32 accuracy from TF32 inputs) with two MMAs per 8-value K
+// step: A_hi [B_hi | B_lo] (N = 64) and A_lo B_hi (N = 32, onto the first 32
+// columns); the epilogue adds the two 32-column halves.
 //
-// One CTA (128 threads) owns 128 rows (one UMMA M=128 tile) and 16 right-
-// hand sides over one K-chunk; it stages 16 complex K-columns at a time into
-// two shared-memory buffers while the tensor core consumes the previous one.
+// A tile is 128 rows (one UMMA M=128 accumulator) x 16 right-hand sides over
+// one K-chunk, consumed in stages of 16 complex K-columns.  The kernels are
+// persistent (one CTA per SM walks the tiles blockIdx.x, blockIdx.x + grid,
+// ...) and warp-specialized, with mbarriers between the roles:
+//   loaders (8 warps)   global loads of stage g + kAhead into registers while
+//                       stage g is split into tf32 head/tail planes (128-byte
+//                       swizzled K-major layout, kPlaneSets buffers)
+//   MMA (1 thread)      tcgen05.mma per stage into one of kAccs TMEM
+//                       accumulators (round robin by tile)
+//   epilogue (4 warps)  TMEM -> registers, split-K reduction, and the result
+//                       through shared memory so that its global accesses
+//                       are coalesced; meanwhile it sets up the accumulator
+//                       of the tile kAccs ahead, so its global latency never
+//                       holds up the tensor core.
 // Every wait on an mbarrier is bounded; a timeout sets bit 2 of the status
-// word, releases tensor memory and leaves the tile unwritten.
+// word and a shared abort flag that ends every role's loop; the CTA then
+// frees tensor memory and returns, leaving unfinished tiles unwritten.
 #include "kernels.cuh"
 #include "umma.cuh"
 
@@ -23,301 +37,599 @@ namespace psp_b200 {
 
 namespace {
 
-using umma::KMajorOffset;
+constexpr int kEpiWarps = 4, kLoadWarps = 8;
+constexpr int kEpiThreads = 32 * kEpiWarps;
+constexpr int kLoadThreads = 32 * kLoadWarps;
+constexpr int kLoad0 = kEpiThreads;                   // first loader thread
+constexpr int kMma0 = kLoad0 + kLoadThreads;          // the MMA thread
+constexpr int kTcThreads = kMma0 + 32;                // 416
 
-constexpr int kTcThreads = 128;
-constexpr int kStageK = 16;                                      // complex K per stage
-constexpr uint32_t kSbo = (2 * kStageK / 4) * umma::kChunkBytes;  // 8-row group stride (1 KB)
-constexpr uint32_t kAPlane = kTcRows * 2 * kStageK * 4;           // 16 KB
-constexpr uint32_t kBPlane = 2 * kSweepCols * 2 * kStageK * 4;    // 4 KB
-constexpr uint32_t kStageBytes = 2 * kAPlane + 2 * kBPlane;
-constexpr int kStages = 2;
-constexpr uint32_t kTmemCols = 32;
-constexpr uint32_t kIdesc = umma::InstrDescTf32(kTcRows, 2 * kSweepCols);
+constexpr int kStageK = 16;                            // complex K per stage (one 128-byte swizzle row)
+constexpr uint32_t kAPlane = kTcRows * 128;            // 16 KB
+constexpr uint32_t kBPlane = 2 * kSweepCols * 128;     // 4 KB: 32 rows
+constexpr uint32_t kPlaneSet = 2 * kAPlane + 2 * kBPlane;  // A hi, A lo, B hi, B lo (B lo right after B hi)
+constexpr int kPlaneSets = 3;
+constexpr int kAhead = 3;                              // stages of copies in flight per loader thread
+constexpr uint32_t kAccCols = 4 * kSweepCols;          // f32 columns per accumulator (two halves)
+constexpr int kAccs = 4;                               // accumulators (tiles in flight per CTA)
+constexpr uint32_t kTmemCols = kAccs * kAccCols;
+constexpr uint32_t kIdescN64 = umma::InstrDescTf32(kTcRows, 4 * kSweepCols);
+constexpr uint32_t kIdescN32 = umma::InstrDescTf32(kTcRows, 2 * kSweepCols);
 
-__device__ __forceinline__ void StoreSplitPair(unsigned char* hi, unsigned char* lo, uint32_t off, float a, float b) {
-    float ah, al, bh, bl;
-    umma::SplitTf32(a, ah, al);
-    umma::SplitTf32(b, bh, bl);
-    *reinterpret_cast<float2*>(hi + off) = make_float2(ah, bh);
-    *reinterpret_cast<float2*>(lo + off) = make_float2(al, bl);
-}
+// A-values per loader thread and stage: forward, thread (row, half) takes 8
+// consecutive K-columns of its row; backward, 16 consecutive threads take
+// the 16 K-values of one row (coalesced along a column of G).
+constexpr int kAPerThread = kStageK * kTcRows / kLoadThreads;  // 8
 
-// B' rows 2n, 2n+1 for complex entry b at (kc, n): the 2x2 real block.
-__device__ __forceinline__ void StoreBBlock(unsigned char* S, int kc, int n, c32 b) {
-    unsigned char* hi = S + 2 * kAPlane;
-    unsigned char* lo = hi + kBPlane;
-    StoreSplitPair(hi, lo, KMajorOffset(2 * n, 2 * kc, kSbo), b.re, -b.im);
-    StoreSplitPair(hi, lo, KMajorOffset(2 * n + 1, 2 * kc, kSbo), b.im, b.re);
-}
+// The result tile passes through shared memory with row stride kOutPad.
+constexpr int kOutPad = kSweepCols + 1;
+constexpr uint32_t kStaging = kTcRows * kOutPad * 8;
+constexpr int kOutRowsPerPass = kEpiThreads / kSweepCols;  // 8
+constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 
-// One stage's operands held in registers between the global loads and the
-// split/store into shared memory, so the loads of stage st+1 are in flight
-// while stage st is handed to the tensor core.
-constexpr int kBPerThread = kStageK * kSweepCols / kTcThreads;  // 2
-struct StageRegs {
-    c32 a[kStageK];
-    c32 b[kBPerThread];
+// Raw stages in flight, each copied asynchronously by the loader threads
+// that later convert them (every thread reads back only its own copies):
+// A [kc][row] (forward) or [row][kc] (backward), then B [plane][kc][n].
+constexpr int kRaw = kAhead + 1;
+constexpr uint32_t kRawA = kStageK * kTcRows * 8;            // 16 KB
+constexpr uint32_t kRawSlot = kRawA + 3 * kStageK * kSweepCols * 8;  // + 6 KB
+constexpr uint32_t kRawOff = kPlaneSets * kPlaneSet;
+constexpr uint32_t kStagingOff = kRawOff + kRaw * kRawSlot;
+constexpr size_t kTcSmem = kStagingOff + kStaging + 1024;
+
+// Stage description handed from the loaders to the MMA thread.
+struct StageHdr {
+    int valid, st, nst, j;
 };
 
-__device__ __forceinline__ c32 LdgC32(const c32* p) {
-    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
-    return mk(v.x, v.y);
+struct Sync {
+    uint64_t planeFull[kPlaneSets], planeEmpty[kPlaneSets];
+    uint64_t accFull[kAccs], accEmpty[kAccs];
+    StageHdr hdr[kPlaneSets];
+    int rawInfo[kRaw];
+    uint32_t tmem;
+    int abort;
+    int isLast;
+};
+
+// Bounded wait (umma::kWaitLimitNs); false once this or another role gave up.
+__device__ __forceinline__ bool Wait(uint64_t* mbar, uint32_t parity, Sync& S, int* status) {
+    if (umma::MbarTryWait(mbar, parity)) return true;
+    const uint64_t t0 = umma::GlobalTimerNs();
+    for (;;) {
+        if (umma::MbarTryWait(mbar, parity)) return true;
+        if (*reinterpret_cast<volatile int*>(&S.abort)) return false;
+        if (umma::GlobalTimerNs() - t0 > umma::kWaitLimitNs) break;
+    }
+    *reinterpret_cast<volatile int*>(&S.abort) = 1;
+    atomicOr(status, 2);
+    return false;
 }
 
-__device__ __forceinline__ void StoreStage(unsigned char* S, const StageRegs& R, bool rowMajorA) {
-    const int tid = threadIdx.x;
-#pragma unroll
-    for (int i = 0; i < kStageK; ++i) {
-        // forward: this thread's row, K-column i; backward: element tid + 128 i
-        const int m = rowMajorA ? (tid + i * kTcThreads) / kStageK : tid;
-        const int kc = rowMajorA ? (tid + i * kTcThreads) % kStageK : i;
-        StoreSplitPair(S, S + kAPlane, KMajorOffset(m, 2 * kc, kSbo), R.a[i].re, R.a[i].im);
-    }
-#pragma unroll
-    for (int j = 0; j < kBPerThread; ++j) {
-        const int e = tid + j * kTcThreads;
-        StoreBBlock(S, e / kSweepCols, e % kSweepCols, R.b[j]);
-    }
+__device__ __forceinline__ void TileRange(const SweepTile& t, bool fwd, int& kb, int& ke, int& nst) {
+    // inv(L11) is lower triangular: the forward K range ends at the tile's
+    // last row, the backward (G^T) range starts at its first
+    kb = fwd ? t.k0 : max(t.k0, t.row0);
+    ke = fwd ? min(t.k1, t.row0 + kTcRows) : t.k1;
+    // an empty range still takes one (zero-filled) stage, so every tile
+    // produces an accumulator
+    nst = ke > kb ? (ke - kb + kStageK - 1) / kStageK : 1;
 }
 
-__device__ __forceinline__ void IssueStage(unsigned char* S, uint32_t tmem, bool first) {
-    const uint32_t aHi = umma::SmemAddr(S), aLo = aHi + kAPlane;
-    const uint32_t bHi = aHi + 2 * kAPlane, bLo = bHi + kBPlane;
+// Zero, or the entry at p when `pred`: a predicated load whose destination
+// is not read until its consumer needs it, so several stay in flight.
+__device__ __forceinline__ c32 LdgC32If(const c32* p, bool pred) {
+    float x, y;
+    asm volatile(
+        "{\n\t.reg .pred q;\n\t"
+        "setp.ne.b32 q, %3, 0;\n\t"
+        "mov.f32 %0, 0f00000000;\n\t"
+        "mov.f32 %1, 0f00000000;\n\t"
+        "@q ld.global.nc.v2.f32 {%0, %1}, [%2];\n\t}\n"
+        : "=f"(x), "=f"(y)
+        : "l"(p), "r"((int)pred));
+    return mk(x, y);
+}
+
+// ------------------------------------------------------------------ loaders
+
+// A stage's place in the tile sequence, packed as
+// (j << 20) | (nst << 10) | st.
+__device__ __forceinline__ int InfoSt(int info) { return info & 1023; }
+__device__ __forceinline__ int InfoNst(int info) { return (info >> 10) & 1023; }
+__device__ __forceinline__ int InfoJ(int info) { return info >> 20; }
+
+// What the loads of one tile need.
+struct LoadMeta {
+    const c32* G;
+    const c32* B;  // forward: Rb; backward: Z
+    int ld, rows, row0, col0, kb, ke, nst;
+};
+
+// Walks this CTA's (tile, stage) sequence for the copies.  The next tile's
+// descriptor is fetched when a tile starts and its front once the tile's
+// first stage is issued, so that neither stalls the copies.
+template <bool kFwd>
+struct LoadCursor {
+    const SweepFront<float>* fr;
+    const SweepTile* tiles;
+    int n, k;
+    int ti, st, j, gl, total;  // gl: stages issued; total: stages in all (-1 until known)
+    LoadMeta m;
+    int nFront, nRow0, nCol0, nK0, nK1;  // next tile
+    const c32 *nG, *nB;                  // its front
+    int ns, nu, haveNt, haveNf;
+
+    __device__ __forceinline__ void SetMeta(int row0, int col0, int k0, int k1, const c32* G, const c32* B, int s,
+                                            int u) {
+        m.G = G;
+        m.B = B;
+        m.ld = s + u;
+        m.rows = kFwd ? s + u : s;
+        m.row0 = row0;
+        m.col0 = col0;
+        SweepTile t;
+        t.row0 = row0; t.k0 = k0; t.k1 = k1;
+        TileRange(t, kFwd, m.kb, m.ke, m.nst);
+    }
+    __device__ __forceinline__ void Start(const SweepFront<float>* fr_, const SweepTile* tiles_, int n_, int k_) {
+        fr = fr_; tiles = tiles_; n = n_; k = k_;
+        ti = blockIdx.x; j = 0; st = 0; gl = 0;
+        total = ti >= n ? 0 : -1;
+        haveNt = haveNf = 0;
+        if (total == 0) return;
+        const SweepTile t = tiles[ti];
+        const SweepFront<float>& f = fr[t.front];
+        SetMeta(t.row0, t.col0, t.k0, t.k1, f.G, kFwd ? f.Rb : f.Z, f.s, f.u);
+        PrefetchTile();
+    }
+    __device__ __forceinline__ void PrefetchTile() {
+        haveNt = ti + (int)gridDim.x < n;
+        haveNf = 0;
+        if (haveNt) {
+            const SweepTile& t = tiles[ti + gridDim.x];
+            nFront = t.front; nRow0 = t.row0; nCol0 = t.col0; nK0 = t.k0; nK1 = t.k1;
+        }
+    }
+    __device__ __forceinline__ void PrefetchFront() {
+        if (haveNt && !haveNf) {
+            const SweepFront<float>& f = fr[nFront];
+            nG = f.G;
+            nB = kFwd ? f.Rb : f.Z;
+            ns = f.s;
+            nu = f.u;
+            haveNf = 1;
+        }
+    }
+    __device__ __forceinline__ bool Valid(int g) const { return total < 0 || g < total; }
+
+    // Issues this thread's copies of the next stage into its raw slot (and
+    // records the stage's place in `info`), commits one copy group and
+    // advances.
+    __device__ __forceinline__ void Issue(unsigned char* raw, int* info) {
+        const int slot = gl % kRaw;
+        if (total >= 0) {
+            umma::CpAsyncCommit();
+            return;
+        }
+        if (threadIdx.x == kLoad0) info[slot] = (j << 20) | (m.nst << 10) | st;
+        const int lt = threadIdx.x - kLoad0;
+        const int kBase = m.kb + st * kStageK;
+        const int ncol = min(kSweepCols, k - m.col0);
+        c32* ra = reinterpret_cast<c32*>(raw + slot * kRawSlot);
+        c32* rb = reinterpret_cast<c32*>(raw + slot * kRawSlot + kRawA);
+        const int kc = lt / kSweepCols, nn = lt % kSweepCols;
+        const int kkB = kBase + kc;
+        const bool bOk = kkB < m.ke && nn < ncol;
+        if (kFwd) {
+            const int row = lt % kTcRows, half = lt / kTcRows;
+            const int r = m.row0 + row;
+            const bool rowOk = r < m.rows;
+#pragma unroll
+            for (int i = 0; i < kAPerThread; ++i) {
+                const int kcA = half * kAPerThread + i, kk = kBase + kcA;
+                const bool ok = rowOk && kk < m.ke;
+                umma::CpAsync8(ra + kcA * kTcRows + row, ok ? m.G + r + (int64_t)kk * m.ld : m.G, ok ? 8u : 0u);
+            }
+            const c32* src = m.B + (int64_t)kkB * 3 * k + m.col0 + nn;
+#pragma unroll
+            for (int p = 0; p < 3; ++p)
+                umma::CpAsync8(rb + p * kStageK * kSweepCols + lt, bOk ? src + p * k : m.B, bOk ? 8u : 0u);
+        } else {
+#pragma unroll
+            for (int i = 0; i < kAPerThread; ++i) {
+                const int e = lt + i * kLoadThreads;
+                const int mm = e / kStageK, kcA = e % kStageK;
+                const int rr = m.row0 + mm, kk = kBase + kcA;
+                const bool ok = rr < m.rows && kk < m.ke;
+                umma::CpAsync8(ra + e, ok ? m.G + kk + (int64_t)rr * m.ld : m.G, ok ? 8u : 0u);
+            }
+            umma::CpAsync8(rb + lt, bOk ? m.B + (int64_t)kkB * k + m.col0 + nn : m.B, bOk ? 8u : 0u);
+        }
+        umma::CpAsyncCommit();
+        ++gl;
+        // advance
+        if (++st < m.nst) {
+            if (st == 1) PrefetchFront();
+            return;
+        }
+        ti += gridDim.x;
+        ++j;
+        st = 0;
+        if (ti >= n) { total = gl; return; }
+        PrefetchFront();
+        SetMeta(nRow0, nCol0, nK0, nK1, nG, nB, ns, nu);
+        PrefetchTile();
+    }
+};
+
+// Splits x into tf32 head and tail.
+__device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
+    umma::SplitTf32(x.re, hi.x, lo.x);
+    umma::SplitTf32(x.im, hi.y, lo.y);
+}
+
+// Converts this thread's copies of one raw stage into plane set P.
+template <bool kFwd>
+__device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawSlot) {
+    const int lt = threadIdx.x - kLoad0;
+    const c32* ra = reinterpret_cast<const c32*>(rawSlot);
+    unsigned char* aHi = P;
+    unsigned char* aLo = P + kAPlane;
+    if (kFwd) {
+        const int row = lt % kTcRows, half = lt / kTcRows;
+#pragma unroll
+        for (int i = 0; i < kAPerThread / 2; ++i) {  // chunk: complex K 2q, 2q+1
+            const int q = half * (kAPerThread / 2) + i;
+            float2 h0, l0, h1, l1;
+            Split2(ra[(2 * q) * kTcRows + row], h0, l0);
+            Split2(ra[(2 * q + 1) * kTcRows + row], h1, l1);
+            const uint32_t off = umma::Sw128Offset(row, q);
+            *reinterpret_cast<float4*>(aHi + off) = make_float4(h0.x, h0.y, h1.x, h1.y);
+            *reinterpret_cast<float4*>(aLo + off) = make_float4(l0.x, l0.y, l1.x, l1.y);
+        }
+    } else {
+        // lanes 2i, 2i+1 hold complex K 2q, 2q+1 of one row: the even lane
+        // writes the chunk's head, the odd lane its tail
+        const bool odd = (threadIdx.x & 1) != 0;
+#pragma unroll
+        for (int i = 0; i < kAPerThread; ++i) {
+            const int e = lt + i * kLoadThreads;
+            const int m = e / kStageK, kc = e % kStageK;
+            float2 h, l;
+            Split2(ra[e], h, l);
+            const float2 send = odd ? h : l;
+            float2 recv;
+            recv.x = __shfl_xor_sync(0xffffffffu, send.x, 1);
+            recv.y = __shfl_xor_sync(0xffffffffu, send.y, 1);
+            const uint32_t off = umma::Sw128Offset(m, kc >> 1);
+            if (odd) *reinterpret_cast<float4*>(aLo + off) = make_float4(recv.x, recv.y, l.x, l.y);
+            else *reinterpret_cast<float4*>(aHi + off) = make_float4(h.x, h.y, recv.x, recv.y);
+        }
+    }
+    // B: entry (kc, n) becomes rows 2n, 2n+1 of B' at K positions 2kc, 2kc+1
+    const int kc = lt / kSweepCols, nn = lt % kSweepCols;
+    const c32* rb = reinterpret_cast<const c32*>(rawSlot + kRawA) + lt;
+    const c32 b = kFwd ? rb[0] + rb[kStageK * kSweepCols] + rb[2 * kStageK * kSweepCols] : rb[0];
+    float2 h, l;
+    Split2(b, h, l);
+    unsigned char* bHi = P + 2 * kAPlane;
+    unsigned char* bLo = bHi + kBPlane;
+    const uint32_t o0 = umma::Sw128Offset(2 * nn, kc >> 1) + (kc & 1) * 8;
+    const uint32_t o1 = umma::Sw128Offset(2 * nn + 1, kc >> 1) + (kc & 1) * 8;
+    *reinterpret_cast<float2*>(bHi + o0) = make_float2(h.x, -h.y);
+    *reinterpret_cast<float2*>(bHi + o1) = make_float2(h.y, h.x);
+    *reinterpret_cast<float2*>(bLo + o0) = make_float2(l.x, -l.y);
+    *reinterpret_cast<float2*>(bLo + o1) = make_float2(l.y, l.x);
+}
+
+// Converts stage g (or ends the stream); false when the role is done.
+template <bool kFwd>
+__device__ __forceinline__ bool LoaderStep(unsigned char* smem, const LoadCursor<kFwd>& cur, int g, Sync& S,
+                                           int* status) {
+    const int ps = g % kPlaneSets;
+    const bool valid = cur.Valid(g);
+    if (g >= kPlaneSets && !Wait(&S.planeEmpty[ps], ((g / kPlaneSets) - 1) & 1, S, status)) return false;
+    umma::CpAsyncWait<kAhead>();  // this thread's copies of stage g have landed
+    if (valid) ConvertStage<kFwd>(smem + ps * kPlaneSet, smem + kRawOff + (g % kRaw) * kRawSlot);
+    umma::FenceProxyAsync();
+    if (threadIdx.x == kLoad0) {
+        const int info = S.rawInfo[g % kRaw];
+        S.hdr[ps] = valid ? StageHdr{1, InfoSt(info), InfoNst(info), InfoJ(info)} : StageHdr{0, 0, 0, 0};
+    }
+    umma::MbarArrive(&S.planeFull[ps]);
+    return valid;
+}
+
+template <bool kFwd>
+__device__ void LoaderRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
+                           int k, unsigned char* smem, Sync& S, int* status) {
+    LoadCursor<kFwd> cur;
+    cur.Start(fr, tiles, n, k);
+    unsigned char* raw = smem + kRawOff;
+#pragma unroll
+    for (int a = 0; a < kAhead; ++a) cur.Issue(raw, S.rawInfo);
+    for (int g = 0;; ++g) {
+        cur.Issue(raw, S.rawInfo);
+        if (!LoaderStep<kFwd>(smem, cur, g, S, status)) break;
+    }
+    umma::CpAsyncWaitAll();
+}
+
+// ------------------------------------------------------------------ MMA
+
+// `init`: the accumulator starts from its current contents (the forward
+// epilogue preloads it); otherwise the tile's first MMA overwrites it.
+__device__ __forceinline__ void IssueStage(const unsigned char* P, uint32_t tmem, bool init) {
+    const uint32_t aHi = umma::SmemAddr(P), aLo = aHi + kAPlane, bHi = aHi + 2 * kAPlane;
 #pragma unroll
     for (int s = 0; s < 2 * kStageK / 8; ++s) {
-        const uint32_t o = s * 2 * umma::kChunkBytes;
-        const uint64_t ah = umma::SmemDesc(aHi + o, umma::kChunkBytes, kSbo);
-        const uint64_t al = umma::SmemDesc(aLo + o, umma::kChunkBytes, kSbo);
-        const uint64_t bh = umma::SmemDesc(bHi + o, umma::kChunkBytes, kSbo);
-        const uint64_t bl = umma::SmemDesc(bLo + o, umma::kChunkBytes, kSbo);
-        umma::MmaTf32(tmem, ah, bh, kIdesc, (first && s == 0) ? 0u : 1u);
-        umma::MmaTf32(tmem, ah, bl, kIdesc, 1u);
-        umma::MmaTf32(tmem, al, bh, kIdesc, 1u);
+        const uint32_t o = s * 32;
+        const uint64_t bd = umma::SmemDescSw128(bHi + o);
+        umma::MmaTf32(tmem, umma::SmemDescSw128(aHi + o), bd, kIdescN64, (init || s > 0) ? 1u : 0u);
+        umma::MmaTf32(tmem, umma::SmemDescSw128(aLo + o), bd, kIdescN32, 1u);
     }
 }
 
-// Split-K over CTAs for 128-row tiles (every thread owns one row).
-__device__ __forceinline__ bool ReduceSplitsTc(const SweepTile& t, const SweepWork& w, c32 (&acc)[kSweepCols]) {
+template <bool kFwd>
+__device__ void MmaRole(const unsigned char* planes, Sync& S, int* status) {
+    for (int g = 0;; ++g) {
+        const int ps = g % kPlaneSets;
+        if (!Wait(&S.planeFull[ps], (g / kPlaneSets) & 1, S, status)) return;
+        const StageHdr h = S.hdr[ps];
+        if (!h.valid) return;  // the epilogue counts its own tiles
+        const int b = h.j % kAccs;
+        if (h.st == 0 && !Wait(&S.accEmpty[b], (h.j / kAccs) & 1, S, status)) return;
+        umma::FenceAfterSync();
+        IssueStage(planes + ps * kPlaneSet, S.tmem + b * kAccCols, kFwd || h.st > 0);
+        umma::CommitTo(&S.planeEmpty[ps]);
+        if (h.st == h.nst - 1) umma::CommitTo(&S.accFull[b]);
+    }
+}
+
+// ------------------------------------------------------------------ epilogue
+
+// Split-K over CTAs: partial tiles [slot][column][row]; the last CTA to arrive
+// sums them in split order.  Epilogue threads only (named barrier 1).
+__device__ __forceinline__ bool ReduceSplitsTc(const SweepTile& t, const SweepWork& w, Sync& S,
+                                               c32 (&acc)[kSweepCols]) {
     if (t.nsplit <= 1) return true;
-    __shared__ int isLast;
     c32* part = reinterpret_cast<c32*>(w.partials);
-    const int tid = threadIdx.x;
+    const int row = threadIdx.x;
     c32* mine = part + ((int64_t)(t.slot + t.split) * kSweepCols) * kTcRows;
 #pragma unroll
-    for (int n = 0; n < kSweepCols; ++n) mine[n * kTcRows + tid] = acc[n];
+    for (int n = 0; n < kSweepCols; ++n) mine[n * kTcRows + row] = acc[n];
     __threadfence();
-    __syncthreads();
-    if (tid == 0) isLast = (atomicAdd(w.counters + t.counter, 1) == t.nsplit - 1);
-    __syncthreads();
-    if (!isLast) return false;
+    umma::NamedBarrier(1, kEpiThreads);
+    if (row == 0) S.isLast = (atomicAdd(w.counters + t.counter, 1) == t.nsplit - 1);
+    umma::NamedBarrier(1, kEpiThreads);
+    const bool last = S.isLast;
+    umma::NamedBarrier(1, kEpiThreads);  // isLast is rewritten by the next tile
+    if (!last) return false;
     __threadfence();
 #pragma unroll
     for (int n = 0; n < kSweepCols; ++n) acc[n] = mk<float>(0, 0);
     for (int s = 0; s < t.nsplit; ++s) {
         const c32* p = part + ((int64_t)(t.slot + s) * kSweepCols) * kTcRows;
 #pragma unroll
-        for (int n = 0; n < kSweepCols; ++n) acc[n] += p[n * kTcRows + tid];
+        for (int n = 0; n < kSweepCols; ++n) acc[n] += p[n * kTcRows + row];
     }
-    if (tid == 0) w.counters[t.counter] = 0;
+    if (row == 0) w.counters[t.counter] = 0;
     return true;
 }
 
-// Shared prologue: mbarriers and TMEM; returns the TMEM base column address.
-__device__ __forceinline__ uint32_t TcSetup(uint64_t* mbar, uint32_t* slot) {
-    const int warp = threadIdx.x / 32;
+// The epilogue keeps kAccs tiles in flight: while tile j's result is
+// written out, the accumulator it used is set up for tile j + kAccs (the
+// forward product starts from the update rows' own right-hand sides, which
+// are carried to the parent; every other entry starts at zero).  Thread e of
+// the epilogue handles column e % 16 of rows e / 16 + 8 i for global
+// accesses and TMEM lane (row) e for tensor memory; the two meet in the
+// shared-memory staging tile.
+
+__device__ __forceinline__ bool TileOf(const SweepTile* tiles, int n, int j, int& ti) {
+    ti = blockIdx.x + j * gridDim.x;
+    return ti < n;
+}
+
+// Loads (coalesced) the forward carry of tile ti: sum of the three
+// right-hand-side planes of the update rows, split 0 only.
+__device__ __forceinline__ void LoadCarry(const SweepFront<float>* fr, const SweepTile* tiles, int ti, int k,
+                                          c32 (&carry)[kOutPerThread]) {
+    const SweepTile t = tiles[ti];
+    const SweepFront<float> f = fr[t.front];
+    const int e = threadIdx.x, n = e % kSweepCols;
+    const bool on = t.split == 0 && f.parentRb && t.col0 + n < k;
+#pragma unroll
+    for (int i = 0; i < kOutPerThread; ++i) {
+        const int r = t.row0 + e / kSweepCols + i * kOutRowsPerPass;
+        const bool ok = on && r >= f.s && r < f.s + f.u;
+        const c32* src = f.Rb + (int64_t)r * 3 * k + t.col0 + n;
+        carry[i] = LdgC32If(src, ok) + LdgC32If(src + k, ok) + LdgC32If(src + 2 * k, ok);
+    }
+}
+
+// Writes the carry into accumulator b (first 32 columns; the other half zero).
+__device__ __forceinline__ void InitAccumulator(Sync& S, int b, const c32 (&carry)[kOutPerThread], c32* staging) {
+    const int e = threadIdx.x, n = e % kSweepCols, warp = e / 32;
+#pragma unroll
+    for (int i = 0; i < kOutPerThread; ++i) staging[(e / kSweepCols + i * kOutRowsPerPass) * kOutPad + n] = carry[i];
+    umma::NamedBarrier(1, kEpiThreads);
+    float v[2 * kSweepCols];
+#pragma unroll
+    for (int c = 0; c < kSweepCols; ++c) {
+        const c32 x = staging[e * kOutPad + c];
+        v[2 * c] = x.re;
+        v[2 * c + 1] = x.im;
+    }
+    const uint32_t taddr = S.tmem + b * kAccCols + ((uint32_t)(warp * 32) << 16);
+    umma::TmemStore32(taddr, v);
+#pragma unroll
+    for (int c = 0; c < 2 * kSweepCols; ++c) v[c] = 0.f;
+    umma::TmemStore32(taddr + 2 * kSweepCols, v);
+    umma::NamedBarrier(1, kEpiThreads);  // staging is reused
+}
+
+// Coalesced write-out of a result tile from the staging tile.
+template <bool kFwd>
+__device__ __forceinline__ void StoreTile(const SweepFront<float>& f, const SweepTile& t, int k, const c32* stage,
+                                          z64* B, c32* X, const PanelIO& io) {
+    const int e = threadIdx.x, n = e % kSweepCols;
+    if (t.col0 + n >= k) return;
+    const int rows = kFwd ? f.s + f.u : f.s;
+#pragma unroll 4
+    for (int i = 0; i < kOutPerThread; ++i) {
+        const int row = e / kSweepCols + i * kOutRowsPerPass;
+        const int r = t.row0 + row;
+        if (r >= rows) break;
+        const c32 v = stage[row * kOutPad + n];
+        if (kFwd) {
+            if (r < f.s) f.Y[(int64_t)r * k + t.col0 + n] = v;
+            else if (f.parentRb) f.parentRb[((int64_t)f.rel[r - f.s] * 3 + 1 + f.childSlot) * k + t.col0 + n] = v;
+        } else {
+            X[(int64_t)(f.ndOff + r) * k + t.col0 + n] = v;
+            const int pn = io.ndToNat[f.ndOff + r];
+            const int xy = pn % io.nxy, vl = pn / io.nxy;
+            if (vl < io.padding) continue;
+            z64* dst = B + (xy + (int64_t)(io.nz - 1 - (io.vOffset + vl)) * io.nxy) * io.ldk + t.col0 + n;
+            const z64 val = ccast<double>(v);
+            *dst = io.outAccumulate ? *dst + val : val;
+        }
+    }
+}
+
+template <bool kFwd>
+__device__ void EpilogueRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
+                             int k, const SweepWork& w, c32* staging, Sync& S, z64* B, const PanelIO& io) {
+    const int warp = threadIdx.x / 32, row = threadIdx.x;
+    c32* X = reinterpret_cast<c32*>(w.xnd);
+    int ti;
+    // set up the first kAccs accumulators
+    for (int q = 0; q < kAccs && TileOf(tiles, n, q, ti); ++q) {
+        if (kFwd) {
+            c32 carry[kOutPerThread];
+            LoadCarry(fr, tiles, ti, k, carry);
+            InitAccumulator(S, q, carry, staging);
+            umma::FenceBeforeSync();
+        }
+        umma::MbarArrive(&S.accEmpty[q]);
+    }
+    for (int j = 0; TileOf(tiles, n, j, ti); ++j) {
+        const int b = j % kAccs;
+        const SweepTile t = tiles[ti];
+        const SweepFront<float> f = fr[t.front];
+        int tn;
+        const bool more = TileOf(tiles, n, j + kAccs, tn);
+        c32 carry[kOutPerThread];
+        if (kFwd && more) LoadCarry(fr, tiles, tn, k, carry);
+        // every epilogue thread takes the same branch (they share named barriers)
+        const bool ok = Wait(&S.accFull[b], (j / kAccs) & 1, S, w.status);
+        if (umma::NamedBarrierOr(1, kEpiThreads, !ok)) return;
+        umma::FenceAfterSync();
+        const uint32_t taddr = S.tmem + b * kAccCols + ((uint32_t)(warp * 32) << 16);
+        c32 acc[kSweepCols];
+        {
+            float v[2 * kSweepCols];
+            umma::TmemLoad32(taddr, v);
+#pragma unroll
+            for (int c = 0; c < kSweepCols; ++c) acc[c] = mk(v[2 * c], v[2 * c + 1]);
+            umma::TmemLoad32(taddr + 2 * kSweepCols, v);
+#pragma unroll
+            for (int c = 0; c < kSweepCols; ++c) acc[c] += mk(v[2 * c], v[2 * c + 1]);
+        }
+        if (more) {
+            if (kFwd) InitAccumulator(S, b, carry, staging);
+            umma::FenceBeforeSync();
+            umma::MbarArrive(&S.accEmpty[b]);
+        }
+        if (!ReduceSplitsTc(t, w, S, acc)) continue;
+#pragma unroll
+        for (int c = 0; c < kSweepCols; ++c) staging[row * kOutPad + c] = acc[c];
+        umma::NamedBarrier(1, kEpiThreads);
+        StoreTile<kFwd>(f, t, k, staging, B, X, io);
+        umma::NamedBarrier(1, kEpiThreads);  // staging is rewritten by the next tile
+    }
+}
+
+// ------------------------------------------------------------------ kernels
+
+__device__ __forceinline__ void InitSync(Sync& S) {
     if (threadIdx.x == 0) {
-        for (int i = 0; i <= kStages; ++i) umma::MbarInit(&mbar[i], 1);
+        for (int i = 0; i < kPlaneSets; ++i) {
+            umma::MbarInit(&S.planeFull[i], kLoadThreads);
+            umma::MbarInit(&S.planeEmpty[i], 1);
+        }
+        for (int i = 0; i < kAccs; ++i) {
+            umma::MbarInit(&S.accFull[i], 1);
+            umma::MbarInit(&S.accEmpty[i], kEpiThreads);
+        }
+        S.abort = 0;
         umma::FenceMbarInit();
     }
-    if (warp == 0) umma::TmemAlloc(slot, kTmemCols);
+    if (threadIdx.x / 32 == 0) umma::TmemAlloc(&S.tmem, kTmemCols);
     umma::FenceBeforeSync();
     __syncthreads();
     umma::FenceAfterSync();
-    return *slot;
 }
 
-// Waits for every issued MMA, reads this thread's accumulator row and frees
-// TMEM.  Returns false (status set) if the tensor-core pipeline timed out.
-__device__ __forceinline__ bool TcFinish(uint64_t* mbar, uint32_t tmem, int nst, bool ok, int* status,
-                                         c32 (&acc)[kSweepCols]) {
-    const int warp = threadIdx.x / 32;
-    if (nst > 0) {
-        if (threadIdx.x == 0) umma::CommitTo(&mbar[kStages]);
-        if (!umma::MbarWaitBounded(&mbar[kStages], 0, status)) ok = false;
-    }
-    ok = !__syncthreads_or(!ok);
-    umma::FenceAfterSync();
-#pragma unroll
-    for (int n = 0; n < kSweepCols; ++n) acc[n] = mk<float>(0, 0);
-    if (nst > 0 && ok) {
-        float v[32];
-        umma::TmemLoad32(tmem + ((uint32_t)(warp * 32) << 16), v);
-#pragma unroll
-        for (int n = 0; n < kSweepCols; ++n) acc[n] = mk(v[2 * n], v[2 * n + 1]);
-    }
+__device__ __forceinline__ void Teardown(Sync& S) {
     umma::FenceBeforeSync();
     __syncthreads();
-    if (warp == 0) umma::TmemDealloc(tmem, kTmemCols);
-    return ok;
+    if (threadIdx.x / 32 == 0) {
+        umma::FenceAfterSync();
+        umma::TmemDealloc(S.tmem, kTmemCols);
+    }
 }
 
-__global__ void __launch_bounds__(kTcThreads) sweep_tc_forward_kernel(const SweepFront<float>* __restrict__ fr,
-                                                                      const SweepTile* __restrict__ tiles, int k,
-                                                                      SweepWork work) {
+__device__ __forceinline__ unsigned char* SmemBase() {
     extern __shared__ unsigned char smem_raw[];
-    __shared__ uint64_t mbar[kStages + 1];
-    __shared__ uint32_t tmemSlot;
-    unsigned char* smem = reinterpret_cast<unsigned char*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const SweepTile t = tiles[blockIdx.x];
-    const SweepFront<float> f = fr[t.front];
-    const int tid = threadIdx.x;
-    const int M = f.s + f.u;
-    const int64_t ld = M;
-    const int ncol = min(kSweepCols, k - t.col0);
-    const int kb = t.k0, ke = min(t.k1, t.row0 + kTcRows);  // inv(L11) is lower triangular
-    const int nst = ke > kb ? (ke - kb + kStageK - 1) / kStageK : 0;
-    const uint32_t tmem = TcSetup(mbar, &tmemSlot);
-    bool ok = true;
-    const int r = t.row0 + tid;
-    // rows of G are strided (column-major): thread = row, loop over K
-    auto load = [&](StageRegs& R, int st) {
-        const int kBase = kb + st * kStageK;
-#pragma unroll
-        for (int kc = 0; kc < kStageK; ++kc) {
-            const int kk = kBase + kc;
-            R.a[kc] = (r < M && kk < ke) ? LdgC32(f.G + r + kk * ld) : mk<float>(0, 0);
-        }
-#pragma unroll
-        for (int j = 0; j < kBPerThread; ++j) {
-            const int e = tid + j * kTcThreads;
-            const int kk = kBase + e / kSweepCols, n = e % kSweepCols;
-            c32 b = mk<float>(0, 0);
-            if (kk < ke && n < ncol) {
-                const c32* src = f.Rb + (int64_t)kk * 3 * k + t.col0 + n;
-                b = src[0] + src[k] + src[2 * k];
-            }
-            R.b[j] = b;
-        }
-    };
-    StageRegs cur, nxt;
-    if (nst > 0) load(cur, 0);
-    for (int st = 0; st < nst; ++st) {
-        const int buf = st & 1;
-        if (st >= kStages && !umma::MbarWaitBounded(&mbar[buf], ((st >> 1) - 1) & 1, work.status)) ok = false;
-        if (__syncthreads_or(!ok)) { ok = false; break; }
-        unsigned char* S = smem + buf * kStageBytes;
-        StoreStage(S, cur, false);
-        if (st + 1 < nst) load(nxt, st + 1);
-        umma::FenceProxyAsync();
-        __syncthreads();
-        if (tid == 0) {
-            umma::FenceAfterSync();
-            IssueStage(S, tmem, st == 0);
-            umma::CommitTo(&mbar[buf]);
-        }
-        cur = nxt;
-    }
-    c32 acc[kSweepCols];
-    if (!TcFinish(mbar, tmem, nst, ok, work.status, acc)) return;
-    if (!ReduceSplitsTc(t, work, acc)) return;
-    if (r >= M) return;
-    if (r < f.s) {
-        c32* dst = f.Y + (int64_t)r * k + t.col0;
-#pragma unroll
-        for (int n = 0; n < kSweepCols; ++n)
-            if (n < ncol) dst[n] = acc[n];
-    } else if (f.parentRb) {
-        const c32* src = f.Rb + (int64_t)r * 3 * k + t.col0;
-        c32* dst = f.parentRb + ((int64_t)f.rel[r - f.s] * 3 + 1 + f.childSlot) * k + t.col0;
-#pragma unroll
-        for (int n = 0; n < kSweepCols; ++n)
-            if (n < ncol) dst[n] = acc[n] + src[n] + src[k + n] + src[2 * k + n];
-    }
+    return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 }
 
-__global__ void __launch_bounds__(kTcThreads) sweep_tc_backward_kernel(const SweepFront<float>* __restrict__ fr,
-                                                                       const SweepTile* __restrict__ tiles,
-                                                                       z64* __restrict__ B, int k, PanelIO io,
-                                                                       SweepWork work) {
-    extern __shared__ unsigned char smem_raw[];
-    __shared__ uint64_t mbar[kStages + 1];
-    __shared__ uint32_t tmemSlot;
-    unsigned char* smem = reinterpret_cast<unsigned char*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    c32* X = reinterpret_cast<c32*>(work.xnd);
-    const SweepTile t = tiles[blockIdx.x];
-    const SweepFront<float> f = fr[t.front];
+__global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const SweepFront<float>* __restrict__ fr,
+                                                                         const SweepTile* __restrict__ tiles, int n,
+                                                                         int k, SweepWork work) {
+    __shared__ Sync S;
+    unsigned char* smem = SmemBase();
+    InitSync(S);
     const int tid = threadIdx.x;
-    const int64_t ld = f.s + f.u;
-    const int ncol = min(kSweepCols, k - t.col0);
-    const int kb = max(t.k0, t.row0), ke = t.k1;  // G^T is upper triangular in its first s columns
-    const int nst = ke > kb ? (ke - kb + kStageK - 1) / kStageK : 0;
-    const uint32_t tmem = TcSetup(mbar, &tmemSlot);
-    bool ok = true;
-    // rows of G^T are contiguous: consecutive threads read consecutive K
-    auto load = [&](StageRegs& R, int st) {
-        const int kBase = kb + st * kStageK;
-#pragma unroll
-        for (int i = 0; i < kStageK; ++i) {
-            const int e = tid + i * kTcThreads;
-            const int rr = t.row0 + e / kStageK, kk = kBase + e % kStageK;
-            R.a[i] = (rr < f.s && kk < ke) ? LdgC32(f.G + kk + rr * ld) : mk<float>(0, 0);
-        }
-#pragma unroll
-        for (int j = 0; j < kBPerThread; ++j) {
-            const int e = tid + j * kTcThreads;
-            const int kk = kBase + e / kSweepCols, n = e % kSweepCols;
-            R.b[j] = (kk < ke && n < ncol) ? f.Z[(int64_t)kk * k + t.col0 + n] : mk<float>(0, 0);
-        }
-    };
-    StageRegs cur, nxt;
-    if (nst > 0) load(cur, 0);
-    for (int st = 0; st < nst; ++st) {
-        const int buf = st & 1;
-        if (st >= kStages && !umma::MbarWaitBounded(&mbar[buf], ((st >> 1) - 1) & 1, work.status)) ok = false;
-        if (__syncthreads_or(!ok)) { ok = false; break; }
-        unsigned char* S = smem + buf * kStageBytes;
-        StoreStage(S, cur, true);
-        if (st + 1 < nst) load(nxt, st + 1);
-        umma::FenceProxyAsync();
-        __syncthreads();
-        if (tid == 0) {
-            umma::FenceAfterSync();
-            IssueStage(S, tmem, st == 0);
-            umma::CommitTo(&mbar[buf]);
-        }
-        cur = nxt;
+    if (tid < kLoad0) {
+        EpilogueRole<true>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + kStagingOff), S, nullptr, PanelIO{});
+    } else if (tid < kMma0) {
+        LoaderRole<true>(fr, tiles, n, k, smem, S, work.status);
+    } else if (tid == kMma0) {
+        MmaRole<true>(smem, S, work.status);
     }
-    c32 acc[kSweepCols];
-    if (!TcFinish(mbar, tmem, nst, ok, work.status, acc)) return;
-    if (!ReduceSplitsTc(t, work, acc)) return;
-    const int r = t.row0 + tid;
-    if (r >= f.s) return;
-    const int col = f.ndOff + r;
-    c32* xd = X + (int64_t)col * k + t.col0;
-#pragma unroll
-    for (int n = 0; n < kSweepCols; ++n)
-        if (n < ncol) xd[n] = acc[n];
-    const int pn = io.ndToNat[col];
-    const int xy = pn % io.nxy, vl = pn / io.nxy;
-    if (vl < io.padding) return;
-    const int v = io.vOffset + vl;
-    z64* dst = B + (xy + (int64_t)(io.nz - 1 - v) * io.nxy) * io.ldk + t.col0;
-#pragma unroll
-    for (int n = 0; n < kSweepCols; ++n) {
-        if (n >= ncol) break;
-        const z64 val = ccast<double>(acc[n]);
-        dst[n] = io.outAccumulate ? dst[n] + val : val;
-    }
+    Teardown(S);
 }
 
-constexpr size_t kTcSmem = kStages * kStageBytes + 1024;
+__global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const SweepFront<float>* __restrict__ fr,
+                                                                          const SweepTile* __restrict__ tiles, int n,
+                                                                          z64* __restrict__ B, int k, PanelIO io,
+                                                                          SweepWork work) {
+    __shared__ Sync S;
+    unsigned char* smem = SmemBase();
+    InitSync(S);
+    const int tid = threadIdx.x;
+    if (tid < kLoad0) {
+        EpilogueRole<false>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + kStagingOff), S, B, io);
+    } else if (tid < kMma0) {
+        LoaderRole<false>(fr, tiles, n, k, smem, S, work.status);
+    } else if (tid == kMma0) {
+        MmaRole<false>(smem, S, work.status);
+    }
+    Teardown(S);
+}
+
+int g_numSMs = 0;
+
+int GridFor(int n) { return n < g_numSMs ? n : g_numSMs; }
 
 }  // namespace
 
 void PrepareSweepTcKernels() {
+    int dev = 0;
+    CUDA_CHECK(cudaGetDevice(&dev));
+    CUDA_CHECK(cudaDeviceGetAttribute(&g_numSMs, cudaDevAttrMultiProcessorCount, dev));
     CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kTcSmem));
     CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -327,14 +639,14 @@ void PrepareSweepTcKernels() {
 void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, const SweepWork& w,
                           cudaStream_t st) {
     if (n <= 0) return;
-    sweep_tc_forward_kernel<<<n, kTcThreads, kTcSmem, st>>>(fr, tiles, k, w);
+    sweep_tc_forward_kernel<<<GridFor(n), kTcThreads, kTcSmem, st>>>(fr, tiles, n, k, w);
     CUDA_LAUNCH_CHECK();
 }
 
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k,
                            const PanelIO& io, const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    sweep_tc_backward_kernel<<<n, kTcThreads, kTcSmem, st>>>(fr, tiles, B, k, io, w);
+    sweep_tc_backward_kernel<<<GridFor(n), kTcThreads, kTcSmem, st>>>(fr, tiles, n, B, k, io, w);
     CUDA_LAUNCH_CHECK();
 }
 

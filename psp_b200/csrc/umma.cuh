@@ -39,6 +39,25 @@ __device__ __forceinline__ uint64_t SmemDesc(uint32_t smemAddr, uint32_t lbo, ui
     return d;
 }
 
+// Descriptor of a K-major operand in the 128-byte-swizzle layout: rows of
+// 128 bytes (32 tf32 K values), 8-row atoms of 1 KB (1 KB aligned), and the
+// 16-byte chunk c of row r stored at chunk position c ^ (r % 8).  Advancing
+// the start address by 32 bytes selects the next 8-value K step.
+__device__ __forceinline__ uint64_t SmemDescSw128(uint32_t smemAddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smemAddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;             // leading byte offset (unused by swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;   // stride byte offset: one 8-row atom
+    d |= (uint64_t)1 << 46;             // descriptor version for sm100
+    d |= (uint64_t)2 << 61;             // SWIZZLE_128B
+    return d;
+}
+
+// Byte offset of the 16-byte chunk `chunk` of row `row` in that layout.
+__device__ __forceinline__ uint32_t Sw128Offset(int row, int chunk) {
+    return (uint32_t)(row >> 3) * 1024u + (uint32_t)(row & 7) * 128u + (uint32_t)((chunk ^ (row & 7)) & 7) * 16u;
+}
+
 // Instruction descriptor: D f32, A and B tf32, both K-major, M x N.
 __host__ __device__ constexpr uint32_t InstrDescTf32(int M, int N) {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
@@ -71,23 +90,38 @@ __device__ __forceinline__ void MbarInit(uint64_t* mbar, uint32_t count) {
 }
 __device__ __forceinline__ void FenceMbarInit() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// One bounded test of a phase; the hardware may suspend the thread (up to
+// about a microsecond) until the phase completes instead of spinning.
 __device__ __forceinline__ bool MbarTryWait(uint64_t* mbar, uint32_t phase) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
         : "=r"(ok)
-        : "r"(SmemAddr(mbar)), "r"(phase)
+        : "r"(SmemAddr(mbar)), "r"(phase), "r"(1000u)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait for `phase` of `mbar`; false (and *status set) on timeout.
+__device__ __forceinline__ uint64_t GlobalTimerNs() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Longest wait on one mbarrier phase before a kernel gives up (ns).
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+// Bounded wait for the phase of parity `phase` of `mbar` to complete; false
+// (and *status set) after kWaitLimitNs.
 __device__ __forceinline__ bool MbarWaitBounded(uint64_t* mbar, uint32_t phase, int* status) {
-    constexpr uint32_t kMaxTries = 1u << 22;
-    for (uint32_t i = 0; i < kMaxTries; ++i)
+    if (MbarTryWait(mbar, phase)) return true;
+    const uint64_t t0 = GlobalTimerNs();
+    for (;;) {
         if (MbarTryWait(mbar, phase)) return true;
+        if (GlobalTimerNs() - t0 > kWaitLimitNs) break;
+    }
     if (status) atomicOr(status, 2);
     return false;
 }
@@ -118,6 +152,81 @@ __device__ __forceinline__ void TmemLoad32(uint32_t taddr, float (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 8-byte asynchronous global->shared copy (no register staging); bytes past
+// `srcBytes` (0 or 8) are zero-filled and not read.
+__device__ __forceinline__ void CpAsync8(void* dst, const void* src, uint32_t srcBytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(SmemAddr(dst)), "l"(src), "r"(srcBytes)
+                 : "memory");
+}
+__device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's committed copy groups are pending.
+template <int N>
+__device__ __forceinline__ void CpAsyncWait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// Arrive on `mbar` once all prior cp.async copies of this thread have landed;
+// the arrival counts against the barrier's initial count.
+__device__ __forceinline__ void CpAsyncArrive(uint64_t* mbar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(SmemAddr(mbar)) : "memory");
+}
+// Plain arrive (release semantics at CTA scope).
+__device__ __forceinline__ void MbarArrive(uint64_t* mbar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(SmemAddr(mbar))
+                 : "memory");
+}
+// Named barrier over `nthreads` threads (a multiple of 32).
+__device__ __forceinline__ void NamedBarrier(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+// Named barrier that also ORs `pred` over the participating threads.
+__device__ __forceinline__ bool NamedBarrierOr(int id, int nthreads, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
+// Writes 32 consecutive f32 columns of this thread's TMEM lane and waits
+// for the write.
+__device__ __forceinline__ void TmemStore32(uint32_t taddr, const float (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n"
+        ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15])),
+        "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])), "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])),
+        "r"(__float_as_uint(v[20])), "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+        "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])), "r"(__float_as_uint(v[27])),
+        "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])), "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// 16 consecutive f32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void TmemLoad16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // Split x into a tf32 head and a tf32 tail: x ~= hi + lo to ~2^-22 relative.
