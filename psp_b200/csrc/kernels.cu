@@ -267,10 +267,10 @@ __global__ void __launch_bounds__(kThreads) ldl_diag_kernel(const FactorFront<R>
         }
     }
     __syncthreads();
-    cpx<R>* Gb = f.G + J + J * ld;
+    cpx<R>* Gb = f.G + J + J * (int64_t)f.ldg;
     for (int e = tid; e < b * b; e += blockDim.x) {
         const int i = e % b, j = e / b;
-        Gb[i + j * ld] = X[i][j];
+        Gb[i + j * (int64_t)f.ldg] = X[i][j];
     }
 }
 
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kThreads) ldl_trsm_kernel(const FactorFront<R>
     const int tid = threadIdx.x;
     for (int e = tid; e < b * b; e += blockDim.x) {
         const int i = e % b, j = e / b;
-        Li[i][j] = f.G[(J + i) + (J + j) * ld];
+        Li[i][j] = f.G[(J + i) + (J + j) * (int64_t)f.ldg];
     }
     if (tid < b) Dinv[tid] = cinv(f.D[J + tid]);
     for (int e = tid; e < rows * b; e += blockDim.x) {

@@ -62,16 +62,22 @@ void LaunchGemm(const GemmOp<R>* ops, const GemmTile* tiles, int numTiles, GemmS
 
 constexpr int kNB = 32;  // column block of the frontal LDL^T
 
+// Leading dimension of a front's persistent factor G: s + u rounded up to
+// even, so that every column starts on a 16-byte boundary for bulk copies
+// (the padding row is zero).
+__host__ __device__ inline int GLeadingDim(int s, int u) { return (s + u + 1) & ~1; }
+
 // One front of one panel during the factorization (cliq::LDL replacement).
 template <typename R>
 struct FactorFront {
     cpx<R>* L;      // transient (s+u) x s frontal columns, ld = s+u
-    cpx<R>* G;      // persistent (s+u) x s: [inv(L11); -L21 inv(L11)], ld = s+u
+    cpx<R>* G;      // persistent (s+u) x s: [inv(L11); -L21 inv(L11)], ld = ldg
     cpx<R>* D;      // persistent pivots, s entries
     cpx<R>* U;      // u x u Schur complement (update matrix), ld = u
     cpx<R>* T;      // inversion scratch
     const int* rel; // u entries: row of each structure index in the parent front
     int s, u;
+    int ldg;        // leading dimension of G: s+u rounded up to even (16-byte aligned columns)
     int parent;     // index of the parent in the same descriptor array (-1 for a root)
     int cls;        // panel class (tables below)
     int ndOff;      // first ND index of the node in its class ordering
@@ -111,7 +117,7 @@ void LaunchLdlTrsm(const FactorFront<R>* fronts, const int2* tasks, int n, int J
 // One front of the panel being solved (cliq::Solve replacement, sweep.cu).
 template <typename R>
 struct SweepFront {
-    const cpx<R>* G;      // (s+u) x s selectively inverted factor, ld = s+u
+    const cpx<R>* G;      // (s+u) x s selectively inverted factor, ld = ldg
     const cpx<R>* D;      // pivots
     cpx<R>* Rb;           // [s+u][3][k]: natural rhs, child 0 update, child 1 update
     cpx<R>* parentRb;     // the parent's Rb (null for a root)
@@ -120,6 +126,7 @@ struct SweepFront {
     const int* lower;     // u ND indices of the front's structure
     const int* rel;       // u rows of the structure in the parent front
     int s, u, ndOff, childSlot;
+    int ldg;              // leading dimension of G (even)
 };
 
 // One CTA of a sweep launch: kSweepRows output rows from row0, kSweepCols

@@ -225,7 +225,7 @@ void FactorStore<R>::Factor() {
         for (int t = 0; t < nn_; ++t) {
             gOff_[(size_t)p * nn_ + t] = gTot;
             dOff_[(size_t)p * nn_ + t] = dTot;
-            gTot += (int64_t)(cs.size[t] + cs.usize[t]) * cs.size[t];
+            gTot += (int64_t)GLeadingDim(cs.size[t], cs.usize[t]) * cs.size[t];
             dTot += cs.size[t];
         }
     }
@@ -247,6 +247,7 @@ void FactorStore<R>::Factor() {
             f.rel = h_.dRel_[c].as<int>() + cs.lowerOff[t];
             f.s = cs.size[t];
             f.u = cs.usize[t];
+            f.ldg = GLeadingDim(f.s, f.u);
             f.parent = tree.nodes[t].parent < 0 ? -1 : p * nn_ + tree.nodes[t].parent;
             f.cls = c;
             f.ndOff = cs.off[t];
@@ -443,11 +444,12 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
                     const int m = a2 - a1, n = a1 - a0;
                     cpx<R>* T = f.T + toff;
                     toff += (int64_t)m * n;
-                    GemmOp<R> op1 = MakeOp<R>(f.L + a1 + a0 * ld, ld, 0, f.G + a0 + a0 * ld, ld, 0, T, m, m, n, n,
+                    const int64_t lg = f.ldg;
+                    GemmOp<R> op1 = MakeOp<R>(f.L + a1 + a0 * ld, ld, 0, f.G + a0 + a0 * lg, lg, 0, T, m, m, n, n,
                                               one, zero);
                     op1.triB = 1;
                     addOp(op1);
-                    GemmOp<R> op2 = MakeOp<R>(f.G + a1 + a1 * ld, ld, 0, T, m, 0, f.G + a1 + a0 * ld, ld, m, n, m,
+                    GemmOp<R> op2 = MakeOp<R>(f.G + a1 + a1 * lg, lg, 0, T, m, 0, f.G + a1 + a0 * lg, lg, m, n, m,
                                               mone, zero);
                     op2.triA = 1;
                     AppendGemmTiles(op2, (int)ops2.size(), kGemmSquare, tiles2);
@@ -464,7 +466,7 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
             const FactorFront<R>& f = all[fi];
             if (f.u == 0) continue;
             const int64_t ld = f.s + f.u;
-            GemmOp<R> g21 = MakeOp<R>(f.L + f.s, ld, 0, f.G, ld, 0, f.G + f.s, ld, f.u, f.s, f.s, mone, zero);
+            GemmOp<R> g21 = MakeOp<R>(f.L + f.s, ld, 0, f.G, f.ldg, 0, f.G + f.s, f.ldg, f.u, f.s, f.s, mone, zero);
             g21.triB = 1;
             addOp(g21);
             GemmOp<R> sch = MakeOp<R>(f.L + f.s, ld, 0, f.L + f.s, ld, 1, f.U, f.u, f.u, f.u, f.s, mone, one);
@@ -565,6 +567,7 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             f.u = cs.usize[t];
             f.ndOff = cs.off[t];
             f.childSlot = (node.parent >= 0 && tree.nodes[node.parent].child[1] == t) ? 1 : 0;
+            f.ldg = GLeadingDim(f.s, f.u);
         }
         P.panelFronts[p] = P.arena.Push(fr);
     }

@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_forward_kernel(const S
     for (int n = 0; n < kSweepCols; ++n) acc[n] = mk<R>(0, 0);
     int sb, se;
     SliceRange(t.k0, t.k1, sb, se);
-    if (r < M) StreamRow<R>(f.G + r, M, sb, min(se, r + 1), t.k0, Bs, acc);  // inv(L11) lower triangular
+    if (r < M) StreamRow<R>(f.G + r, f.ldg, sb, min(se, r + 1), t.k0, Bs, acc);  // inv(L11) lower triangular
     ReduceSlices<R>(Bs, acc);
     if (!ReduceSplits<R>(t, work, acc)) return;
     if (tid >= kSweepRows || r >= M) return;
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) sweep_backward_kernel(const 
     const int tid = threadIdx.x;
     const int kc = t.k1 - t.k0;
     const int ncol = min(kSweepCols, k - t.col0);
-    const int64_t ld = f.s + f.u;
+    const int64_t ld = f.ldg;
     for (int e = tid; e < kc * kSweepCols; e += blockDim.x) {
         const int kk = e / kSweepCols, n = e % kSweepCols;
         Zs[e] = n < ncol ? f.Z[(int64_t)(t.k0 + kk) * k + t.col0 + n] : mk<R>(0, 0);

@@ -17,9 +17,15 @@
 // one K-chunk, consumed in stages of 16 complex K-columns.  The kernels are
 // persistent (one CTA per SM walks the tiles blockIdx.x, blockIdx.x + grid,
 // ...) and warp-specialized, with mbarriers between the roles:
-//   loaders (8 warps)   global loads of stage g + kAhead into registers while
-//                       stage g is split into tf32 head/tail planes (128-byte
-//                       swizzled K-major layout, kPlaneSets buffers)
+//   producer (1 warp)   forward: bulk copies of G's 1 KB column segments
+//                       into a ring of kRaw raw stages (completion by
+//                       transaction bytes)
+//   converters (8 warps) split raw stage g into tf32 head/tail planes
+//                       (128-byte swizzled K-major layout, kPlaneSets
+//                       buffers); each also copies its own right-hand-side
+//                       entries kAhead stages ahead, and in the backward
+//                       (128-byte rows of G^T, too short for bulk copies)
+//                       its own 16-byte chunks of A
 //   MMA (1 thread)      tcgen05.mma per stage into one of kAccs TMEM
 //                       accumulators (round robin by tile)
 //   epilogue (4 warps)  TMEM -> registers, split-K reduction, and the result
@@ -40,26 +46,28 @@ namespace {
 constexpr int kEpiWarps = 4, kLoadWarps = 8;
 constexpr int kEpiThreads = 32 * kEpiWarps;
 constexpr int kLoadThreads = 32 * kLoadWarps;
-constexpr int kLoad0 = kEpiThreads;                   // first loader thread
+constexpr int kLoad0 = kEpiThreads;                   // first converter thread
 constexpr int kMma0 = kLoad0 + kLoadThreads;          // the MMA thread
-constexpr int kTcThreads = kMma0 + 32;                // 416
+constexpr int kProd0 = kMma0 + 32;                    // the producer warp
+constexpr int kTcThreads = kProd0 + 32;               // 448
 
 constexpr int kStageK = 16;                            // complex K per stage (one 128-byte swizzle row)
 constexpr uint32_t kAPlane = kTcRows * 128;            // 16 KB
 constexpr uint32_t kBPlane = 2 * kSweepCols * 128;     // 4 KB: 32 rows
 constexpr uint32_t kPlaneSet = 2 * kAPlane + 2 * kBPlane;  // A hi, A lo, B hi, B lo (B lo right after B hi)
 constexpr int kPlaneSets = 3;
-constexpr int kAhead = 3;                              // stages of copies in flight per loader thread
+constexpr int kAhead = 3;                              // stages of copies in flight
 constexpr uint32_t kAccCols = 4 * kSweepCols;          // f32 columns per accumulator (two halves)
 constexpr int kAccs = 4;                               // accumulators (tiles in flight per CTA)
 constexpr uint32_t kTmemCols = kAccs * kAccCols;
 constexpr uint32_t kIdescN64 = umma::InstrDescTf32(kTcRows, 4 * kSweepCols);
 constexpr uint32_t kIdescN32 = umma::InstrDescTf32(kTcRows, 2 * kSweepCols);
 
-// A-values per loader thread and stage: forward, thread (row, half) takes 8
-// consecutive K-columns of its row; backward, 16 consecutive threads take
-// the 16 K-values of one row (coalesced along a column of G).
+// A-values per converter thread and stage: forward, thread (row, half)
+// takes 8 consecutive K-columns of its row; backward, 16 consecutive threads
+// take the 16 K-values of one row.
 constexpr int kAPerThread = kStageK * kTcRows / kLoadThreads;  // 8
+constexpr int kAChunks = kAPerThread / 2;                       // 16-byte chunks (backward copies)
 
 // The result tile passes through shared memory with row stride kOutPad.
 constexpr int kOutPad = kSweepCols + 1;
@@ -67,9 +75,9 @@ constexpr uint32_t kStaging = kTcRows * kOutPad * 8;
 constexpr int kOutRowsPerPass = kEpiThreads / kSweepCols;  // 8
 constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 
-// Raw stages in flight, each copied asynchronously by the loader threads
-// that later convert them (every thread reads back only its own copies):
-// A [kc][row] (forward) or [row][kc] (backward), then B [plane][kc][n].
+// Raw stages in flight: A arrives by bulk copies of whole column segments
+// of G (forward layout [kc][row], backward [row][kc]); B [plane][kc][n] is
+// copied entry by entry by the converter thread that later reads it.
 constexpr int kRaw = kAhead + 1;
 constexpr uint32_t kRawA = kStageK * kTcRows * 8;            // 16 KB
 constexpr uint32_t kRawSlot = kRawA + 3 * kStageK * kSweepCols * 8;  // + 6 KB
@@ -85,8 +93,10 @@ struct StageHdr {
 struct Sync {
     uint64_t planeFull[kPlaneSets], planeEmpty[kPlaneSets];
     uint64_t accFull[kAccs], accEmpty[kAccs];
+    uint64_t rawFull[kRaw], rawEmpty[kRaw];
     StageHdr hdr[kPlaneSets];
-    int rawInfo[kRaw];
+    int rawInfo[kRaw];      // stage place, packed (see InfoSt); written and read by the first converter
+    int rawK[kRaw][2];      // stage's first K index and the tile's K end
     uint32_t tmem;
     int abort;
     int isLast;
@@ -139,16 +149,16 @@ __device__ __forceinline__ int InfoSt(int info) { return info & 1023; }
 __device__ __forceinline__ int InfoNst(int info) { return (info >> 10) & 1023; }
 __device__ __forceinline__ int InfoJ(int info) { return info >> 20; }
 
-// What the loads of one tile need.
+// What the copies of one tile need.
 struct LoadMeta {
     const c32* G;
     const c32* B;  // forward: Rb; backward: Z
     int ld, rows, row0, col0, kb, ke, nst;
 };
 
-// Walks this CTA's (tile, stage) sequence for the copies.  The next tile's
-// descriptor is fetched when a tile starts and its front once the tile's
-// first stage is issued, so that neither stalls the copies.
+// Walks this CTA's (tile, stage) sequence.  The next tile's descriptor is
+// fetched when a tile starts and its front once the tile's first stage is
+// issued, so that neither stalls the copies.
 template <bool kFwd>
 struct LoadCursor {
     const SweepFront<float>* fr;
@@ -164,7 +174,7 @@ struct LoadCursor {
                                             int u) {
         m.G = G;
         m.B = B;
-        m.ld = s + u;
+        m.ld = GLeadingDim(s, u);
         m.rows = kFwd ? s + u : s;
         m.row0 = row0;
         m.col0 = col0;
@@ -202,53 +212,12 @@ struct LoadCursor {
         }
     }
     __device__ __forceinline__ bool Valid(int g) const { return total < 0 || g < total; }
+    __device__ __forceinline__ int Info() const { return (j << 20) | (m.nst << 10) | st; }
+    __device__ __forceinline__ int KBase() const { return m.kb + st * kStageK; }
 
-    // Issues this thread's copies of the next stage into its raw slot (and
-    // records the stage's place in `info`), commits one copy group and
-    // advances.
-    __device__ __forceinline__ void Issue(unsigned char* raw, int* info) {
-        const int slot = gl % kRaw;
-        if (total >= 0) {
-            umma::CpAsyncCommit();
-            return;
-        }
-        if (threadIdx.x == kLoad0) info[slot] = (j << 20) | (m.nst << 10) | st;
-        const int lt = threadIdx.x - kLoad0;
-        const int kBase = m.kb + st * kStageK;
-        const int ncol = min(kSweepCols, k - m.col0);
-        c32* ra = reinterpret_cast<c32*>(raw + slot * kRawSlot);
-        c32* rb = reinterpret_cast<c32*>(raw + slot * kRawSlot + kRawA);
-        const int kc = lt / kSweepCols, nn = lt % kSweepCols;
-        const int kkB = kBase + kc;
-        const bool bOk = kkB < m.ke && nn < ncol;
-        if (kFwd) {
-            const int row = lt % kTcRows, half = lt / kTcRows;
-            const int r = m.row0 + row;
-            const bool rowOk = r < m.rows;
-#pragma unroll
-            for (int i = 0; i < kAPerThread; ++i) {
-                const int kcA = half * kAPerThread + i, kk = kBase + kcA;
-                const bool ok = rowOk && kk < m.ke;
-                umma::CpAsync8(ra + kcA * kTcRows + row, ok ? m.G + r + (int64_t)kk * m.ld : m.G, ok ? 8u : 0u);
-            }
-            const c32* src = m.B + (int64_t)kkB * 3 * k + m.col0 + nn;
-#pragma unroll
-            for (int p = 0; p < 3; ++p)
-                umma::CpAsync8(rb + p * kStageK * kSweepCols + lt, bOk ? src + p * k : m.B, bOk ? 8u : 0u);
-        } else {
-#pragma unroll
-            for (int i = 0; i < kAPerThread; ++i) {
-                const int e = lt + i * kLoadThreads;
-                const int mm = e / kStageK, kcA = e % kStageK;
-                const int rr = m.row0 + mm, kk = kBase + kcA;
-                const bool ok = rr < m.rows && kk < m.ke;
-                umma::CpAsync8(ra + e, ok ? m.G + kk + (int64_t)rr * m.ld : m.G, ok ? 8u : 0u);
-            }
-            umma::CpAsync8(rb + lt, bOk ? m.B + (int64_t)kkB * k + m.col0 + nn : m.B, bOk ? 8u : 0u);
-        }
-        umma::CpAsyncCommit();
+    // Moves to the next stage.
+    __device__ __forceinline__ void Advance() {
         ++gl;
-        // advance
         if (++st < m.nst) {
             if (st == 1) PrefetchFront();
             return;
@@ -263,48 +232,140 @@ struct LoadCursor {
     }
 };
 
+// ------------------------------------------------------------------ producer
+
+// One warp copies each stage's A operand with bulk copies of contiguous
+// segments of G: forward, up to 16 K-columns of up to 128 rows (rounded up
+// to an even count, which G's even leading dimension keeps inside the
+// column); backward, up to 128 rows of G^T of 16 K-values.  Lane 0 arms the
+// slot's barrier with the byte count before any lane copies.
+template <bool kFwd>
+__device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
+                             int k, unsigned char* raw, Sync& S, int* status) {
+    const int lane = threadIdx.x & 31;
+    LoadCursor<kFwd> cur;
+    cur.Start(fr, tiles, n, k);
+    for (int g = 0; cur.Valid(g); ++g) {
+        const int slot = g % kRaw;
+        if (g >= kRaw && !Wait(&S.rawEmpty[slot], ((g / kRaw) - 1) & 1, S, status)) return;
+        const LoadMeta& m = cur.m;
+        const int kBase = cur.KBase();
+        uint32_t bytes;
+        if (kFwd) {
+            const int rows = min(kTcRows, m.rows - m.row0);
+            const int ncols = min(kStageK, m.ke - kBase);
+            bytes = (ncols > 0 && rows > 0) ? (uint32_t)ncols * (uint32_t)((rows + 1) & ~1) * 8u : 0u;
+        } else {
+            const int rows = min(kTcRows, m.rows - m.row0);
+            const int ncols = min(kStageK, m.ke - kBase);
+            bytes = (ncols > 0 && rows > 0) ? (uint32_t)rows * (uint32_t)((ncols + 1) & ~1) * 8u : 0u;
+        }
+        if (lane == 0) {
+            S.rawK[slot][0] = kBase;
+            S.rawK[slot][1] = m.ke;
+            umma::MbarArriveExpectTx(&S.rawFull[slot], bytes);
+        }
+        __syncwarp();
+        unsigned char* dst = raw + slot * kRawSlot;
+        if (bytes) {
+            if (kFwd) {
+                const int rows2 = (min(kTcRows, m.rows - m.row0) + 1) & ~1;
+                const int ncols = min(kStageK, m.ke - kBase);
+                if (lane < ncols)
+                    umma::BulkCopy(dst + lane * kTcRows * 8, m.G + m.row0 + (int64_t)(kBase + lane) * m.ld,
+                                   (uint32_t)rows2 * 8u, &S.rawFull[slot]);
+            } else {
+                const int rows = min(kTcRows, m.rows - m.row0);
+                const int ncols2 = (min(kStageK, m.ke - kBase) + 1) & ~1;
+                for (int r = lane; r < rows; r += 32)
+                    umma::BulkCopy(dst + r * kStageK * 8, m.G + kBase + (int64_t)(m.row0 + r) * m.ld,
+                                   (uint32_t)ncols2 * 8u, &S.rawFull[slot]);
+            }
+        }
+        cur.Advance();
+    }
+}
+
+// ------------------------------------------------------------------ converters
+
 // Splits x into tf32 head and tail.
 __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
     umma::SplitTf32(x.re, hi.x, lo.x);
     umma::SplitTf32(x.im, hi.y, lo.y);
 }
 
-// Converts this thread's copies of one raw stage into plane set P.
+// Issues this converter thread's own copies of the cursor's stage (its B
+// entry; backward also its four 16-byte A chunks, zero-filled outside the
+// tile), commits one copy group and advances the cursor.
 template <bool kFwd>
-__device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawSlot) {
+__device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* raw, Sync& S) {
+    if (cur.total >= 0) {
+        umma::CpAsyncCommit();
+        return;
+    }
+    const int slot = cur.gl % kRaw;
+    const LoadMeta& m = cur.m;
+    const int lt = threadIdx.x - kLoad0;
+    if (lt == 0) S.rawInfo[slot] = cur.Info();  // read back by this thread for the stage header
+    const int kc = lt / kSweepCols, nn = lt % kSweepCols;
+    const int kk = cur.KBase() + kc;
+    const bool ok = kk < m.ke && nn < min(kSweepCols, cur.k - m.col0);
+    c32* rb = reinterpret_cast<c32*>(raw + slot * kRawSlot + kRawA);
+    if (kFwd) {
+        const c32* src = m.B + (int64_t)kk * 3 * cur.k + m.col0 + nn;
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+            umma::CpAsync8(rb + p * kStageK * kSweepCols + lt, ok ? src + p * cur.k : m.B, ok ? 8u : 0u);
+    } else {
+        umma::CpAsync8(rb + lt, ok ? m.B + (int64_t)kk * cur.k + m.col0 + nn : m.B, ok ? 8u : 0u);
+        c32* ra = reinterpret_cast<c32*>(raw + slot * kRawSlot);
+        const int kBase = cur.KBase();
+#pragma unroll
+        for (int i = 0; i < kAChunks; ++i) {
+            const int c = lt + i * kLoadThreads;
+            const int mm = c / (kStageK / 2), q = c % (kStageK / 2);
+            const int rr = m.row0 + mm, kk0 = kBase + 2 * q;
+            const int nv = (rr < m.rows) ? max(0, min(2, m.ke - kk0)) : 0;
+            umma::CpAsync16(ra + mm * kStageK + 2 * q, nv ? m.G + kk0 + (int64_t)rr * m.ld : m.G, 8u * nv);
+        }
+    }
+    umma::CpAsyncCommit();
+    cur.Advance();
+}
+
+// Converts one raw stage into plane set P; K-columns at or beyond kEnd
+// (relative to the stage's first column kBase) are taken as zero.
+template <bool kFwd>
+__device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawSlot, int kValid) {
     const int lt = threadIdx.x - kLoad0;
     const c32* ra = reinterpret_cast<const c32*>(rawSlot);
     unsigned char* aHi = P;
     unsigned char* aLo = P + kAPlane;
+    const c32 zero = mk<float>(0, 0);
     if (kFwd) {
         const int row = lt % kTcRows, half = lt / kTcRows;
 #pragma unroll
         for (int i = 0; i < kAPerThread / 2; ++i) {  // chunk: complex K 2q, 2q+1
             const int q = half * (kAPerThread / 2) + i;
             float2 h0, l0, h1, l1;
-            Split2(ra[(2 * q) * kTcRows + row], h0, l0);
-            Split2(ra[(2 * q + 1) * kTcRows + row], h1, l1);
+            Split2(2 * q < kValid ? ra[(2 * q) * kTcRows + row] : zero, h0, l0);
+            Split2(2 * q + 1 < kValid ? ra[(2 * q + 1) * kTcRows + row] : zero, h1, l1);
             const uint32_t off = umma::Sw128Offset(row, q);
             *reinterpret_cast<float4*>(aHi + off) = make_float4(h0.x, h0.y, h1.x, h1.y);
             *reinterpret_cast<float4*>(aLo + off) = make_float4(l0.x, l0.y, l1.x, l1.y);
         }
     } else {
-        // lanes 2i, 2i+1 hold complex K 2q, 2q+1 of one row: the even lane
-        // writes the chunk's head, the odd lane its tail
-        const bool odd = (threadIdx.x & 1) != 0;
+        // this thread's own chunks (already zero-filled outside the tile)
 #pragma unroll
-        for (int i = 0; i < kAPerThread; ++i) {
-            const int e = lt + i * kLoadThreads;
-            const int m = e / kStageK, kc = e % kStageK;
-            float2 h, l;
-            Split2(ra[e], h, l);
-            const float2 send = odd ? h : l;
-            float2 recv;
-            recv.x = __shfl_xor_sync(0xffffffffu, send.x, 1);
-            recv.y = __shfl_xor_sync(0xffffffffu, send.y, 1);
-            const uint32_t off = umma::Sw128Offset(m, kc >> 1);
-            if (odd) *reinterpret_cast<float4*>(aLo + off) = make_float4(recv.x, recv.y, l.x, l.y);
-            else *reinterpret_cast<float4*>(aHi + off) = make_float4(h.x, h.y, recv.x, recv.y);
+        for (int i = 0; i < kAChunks; ++i) {
+            const int c = lt + i * kLoadThreads;
+            const int m = c / (kStageK / 2), q = c % (kStageK / 2);
+            float2 h0, l0, h1, l1;
+            Split2(ra[m * kStageK + 2 * q], h0, l0);
+            Split2(ra[m * kStageK + 2 * q + 1], h1, l1);
+            const uint32_t off = umma::Sw128Offset(m, q);
+            *reinterpret_cast<float4*>(aHi + off) = make_float4(h0.x, h0.y, h1.x, h1.y);
+            *reinterpret_cast<float4*>(aLo + off) = make_float4(l0.x, l0.y, l1.x, l1.y);
         }
     }
     // B: entry (kc, n) becomes rows 2n, 2n+1 of B' at K positions 2kc, 2kc+1
@@ -325,33 +386,38 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
 
 // Converts stage g (or ends the stream); false when the role is done.
 template <bool kFwd>
-__device__ __forceinline__ bool LoaderStep(unsigned char* smem, const LoadCursor<kFwd>& cur, int g, Sync& S,
-                                           int* status) {
-    const int ps = g % kPlaneSets;
+__device__ __forceinline__ bool ConverterStep(unsigned char* smem, const LoadCursor<kFwd>& cur, int g, Sync& S,
+                                              int* status) {
+    const int ps = g % kPlaneSets, slot = g % kRaw;
     const bool valid = cur.Valid(g);
+    if (kFwd && valid && !Wait(&S.rawFull[slot], (g / kRaw) & 1, S, status)) return false;
     if (g >= kPlaneSets && !Wait(&S.planeEmpty[ps], ((g / kPlaneSets) - 1) & 1, S, status)) return false;
-    umma::CpAsyncWait<kAhead>();  // this thread's copies of stage g have landed
-    if (valid) ConvertStage<kFwd>(smem + ps * kPlaneSet, smem + kRawOff + (g % kRaw) * kRawSlot);
+    umma::CpAsyncWait<kAhead>();  // this thread's own copies of stage g have landed
+    if (valid) {
+        const int kValid = kFwd ? S.rawK[slot][1] - S.rawK[slot][0] : kStageK;
+        ConvertStage<kFwd>(smem + ps * kPlaneSet, smem + kRawOff + slot * kRawSlot, kValid);
+    }
     umma::FenceProxyAsync();
     if (threadIdx.x == kLoad0) {
-        const int info = S.rawInfo[g % kRaw];
+        const int info = S.rawInfo[slot];
         S.hdr[ps] = valid ? StageHdr{1, InfoSt(info), InfoNst(info), InfoJ(info)} : StageHdr{0, 0, 0, 0};
     }
     umma::MbarArrive(&S.planeFull[ps]);
+    if (kFwd && valid) umma::MbarArrive(&S.rawEmpty[slot]);
     return valid;
 }
 
 template <bool kFwd>
-__device__ void LoaderRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
-                           int k, unsigned char* smem, Sync& S, int* status) {
+__device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
+                              int k, unsigned char* smem, Sync& S, int* status) {
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
     unsigned char* raw = smem + kRawOff;
 #pragma unroll
-    for (int a = 0; a < kAhead; ++a) cur.Issue(raw, S.rawInfo);
+    for (int a = 0; a < kAhead; ++a) IssueOwn(cur, raw, S);
     for (int g = 0;; ++g) {
-        cur.Issue(raw, S.rawInfo);
-        if (!LoaderStep<kFwd>(smem, cur, g, S, status)) break;
+        IssueOwn(cur, raw, S);
+        if (!ConverterStep<kFwd>(smem, cur, g, S, status)) break;
     }
     umma::CpAsyncWaitAll();
 }
@@ -562,6 +628,10 @@ __device__ __forceinline__ void InitSync(Sync& S) {
             umma::MbarInit(&S.accFull[i], 1);
             umma::MbarInit(&S.accEmpty[i], kEpiThreads);
         }
+        for (int i = 0; i < kRaw; ++i) {
+            umma::MbarInit(&S.rawFull[i], 1);
+            umma::MbarInit(&S.rawEmpty[i], kLoadThreads);
+        }
         S.abort = 0;
         umma::FenceMbarInit();
     }
@@ -595,9 +665,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
     if (tid < kLoad0) {
         EpilogueRole<true>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + kStagingOff), S, nullptr, PanelIO{});
     } else if (tid < kMma0) {
-        LoaderRole<true>(fr, tiles, n, k, smem, S, work.status);
+        ConverterRole<true>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
         MmaRole<true>(smem, S, work.status);
+    } else if (tid >= kProd0) {
+        ProducerRole<true>(fr, tiles, n, k, smem + kRawOff, S, work.status);
     }
     Teardown(S);
 }
@@ -613,7 +685,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const 
     if (tid < kLoad0) {
         EpilogueRole<false>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + kStagingOff), S, B, io);
     } else if (tid < kMma0) {
-        LoaderRole<false>(fr, tiles, n, k, smem, S, work.status);
+        ConverterRole<false>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
         MmaRole<false>(smem, S, work.status);
     }

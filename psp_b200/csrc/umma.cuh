@@ -160,6 +160,12 @@ __device__ __forceinline__ void CpAsync8(void* dst, const void* src, uint32_t sr
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(SmemAddr(dst)), "l"(src), "r"(srcBytes)
                  : "memory");
 }
+// 16-byte asynchronous global->shared copy (both addresses 16-byte aligned);
+// bytes past `srcBytes` (0, 8 or 16) are zero-filled and not read.
+__device__ __forceinline__ void CpAsync16(void* dst, const void* src, uint32_t srcBytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(SmemAddr(dst)), "l"(src), "r"(srcBytes)
+                 : "memory");
+}
 __device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // Waits until at most N of this thread's committed copy groups are pending.
 template <int N>
@@ -172,6 +178,23 @@ __device__ __forceinline__ void CpAsyncWaitAll() { asm volatile("cp.async.wait_a
 __device__ __forceinline__ void CpAsyncArrive(uint64_t* mbar) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(SmemAddr(mbar)) : "memory");
 }
+// Bulk asynchronous copy of `bytes` (a multiple of 16; both addresses 16-byte
+// aligned) from global to this CTA's shared memory, completing as
+// transaction bytes on `mbar`.
+__device__ __forceinline__ void BulkCopy(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(SmemAddr(dst)),
+        "l"(src), "r"(bytes), "r"(SmemAddr(mbar))
+        : "memory");
+}
+// Arrive on `mbar` and add `bytes` to the transaction bytes its phase waits for.
+__device__ __forceinline__ void MbarArriveExpectTx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
+                     SmemAddr(mbar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
 // Plain arrive (release semantics at CTA scope).
 __device__ __forceinline__ void MbarArrive(uint64_t* mbar) {
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(SmemAddr(mbar))
