@@ -575,9 +575,10 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // has a few CTAs per SM; rows of a tile share one K range (inv(L11) is
     // triangular, so the forward range stops at the tile's last row and the
     // backward range starts at its first).
-    // Tensor-core CTAs stream their chunk in 16-column stages, one stage per
-    // load latency: short chunks keep CTAs uniform and launches tail-free.
-    const int maxChunk = tc_ ? 128 : SweepMaxChunk<R>();
+    // The tensor-core kernels are persistent and pipeline across tiles, so
+    // long chunks cost nothing extra and save split-K partial sums; the
+    // chunk only shrinks to give every SM tiles.
+    const int maxChunk = tc_ ? 512 : SweepMaxChunk<R>();
     const int tileRows = TileRows();
     int64_t maxSlots = 1, maxCounters = 1;
     auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepTile>& tiles, int& chunk,

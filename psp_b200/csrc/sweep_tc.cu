@@ -50,24 +50,19 @@ constexpr int kLoad0 = kEpiThreads;                   // first converter thread
 constexpr int kMma0 = kLoad0 + kLoadThreads;          // the MMA thread
 constexpr int kProd0 = kMma0 + 32;                    // the producer warp
 constexpr int kTcThreads = kProd0 + 32;               // 448
+constexpr int kGroups = 2;                            // converter groups, alternating stages
+constexpr int kGroupThreads = kLoadThreads / kGroups; // 128
 
 constexpr int kStageK = 16;                            // complex K per stage (one 128-byte swizzle row)
 constexpr uint32_t kAPlane = kTcRows * 128;            // 16 KB
 constexpr uint32_t kBPlane = 2 * kSweepCols * 128;     // 4 KB: 32 rows
 constexpr uint32_t kPlaneSet = 2 * kAPlane + 2 * kBPlane;  // A hi, A lo, B hi, B lo (B lo right after B hi)
-constexpr int kPlaneSets = 3;
-constexpr int kAhead = 3;                              // stages of copies in flight
+constexpr int kPlaneSets = kGroups;                    // one per converter group
 constexpr uint32_t kAccCols = 4 * kSweepCols;          // f32 columns per accumulator (two halves)
 constexpr int kAccs = 4;                               // accumulators (tiles in flight per CTA)
 constexpr uint32_t kTmemCols = kAccs * kAccCols;
 constexpr uint32_t kIdescN64 = umma::InstrDescTf32(kTcRows, 4 * kSweepCols);
 constexpr uint32_t kIdescN32 = umma::InstrDescTf32(kTcRows, 2 * kSweepCols);
-
-// A-values per converter thread and stage: forward, thread (row, half)
-// takes 8 consecutive K-columns of its row; backward, 16 consecutive threads
-// take the 16 K-values of one row.
-constexpr int kAPerThread = kStageK * kTcRows / kLoadThreads;  // 8
-constexpr int kAChunks = kAPerThread / 2;                       // 16-byte chunks (backward copies)
 
 // The result tile passes through shared memory with row stride kOutPad.
 constexpr int kOutPad = kSweepCols + 1;
@@ -75,14 +70,26 @@ constexpr uint32_t kStaging = kTcRows * kOutPad * 8;
 constexpr int kOutRowsPerPass = kEpiThreads / kSweepCols;  // 8
 constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 
-// Raw stages in flight: A arrives by bulk copies of whole column segments
-// of G (forward layout [kc][row], backward [row][kc]); B [plane][kc][n] is
-// copied entry by entry by the converter thread that later reads it.
-constexpr int kRaw = kAhead + 1;
-constexpr uint32_t kRawA = kStageK * kTcRows * 8;            // 16 KB
-constexpr uint32_t kRawSlot = kRawA + 3 * kStageK * kSweepCols * 8;  // + 6 KB
-constexpr uint32_t kRawOff = kPlaneSets * kPlaneSet;
-constexpr uint32_t kStagingOff = kRawOff + kRaw * kRawSlot;
+// Raw data of the stages in flight.
+//   forward:  A (G's column segments, [kc][row]) arrives by bulk copies
+//             into a ring of kRaw slots shared by both groups;
+//   each group: a ring of kOwn slots of its own copies (forward: B
+//             [plane][kc][n]; backward: A [row][kc] then B [kc][n]), every
+//             entry read back by the thread that copied it.
+constexpr int kRaw = 4;
+constexpr int kAheadOwn = 2;                           // own stages in flight per group
+constexpr int kOwn = kAheadOwn + 1;
+constexpr uint32_t kRawA = kStageK * kTcRows * 8;      // 16 KB
+__host__ __device__ constexpr uint32_t OwnSlot(bool fwd) {
+    return fwd ? 3 * kStageK * kSweepCols * 8 : kRawA + kStageK * kSweepCols * 8;
+}
+__host__ __device__ constexpr uint32_t OwnBase(bool fwd) { return fwd ? kRaw * kRawA : 0; }
+constexpr uint32_t kRegionOff = kPlaneSets * kPlaneSet;
+constexpr uint32_t kRegion =
+    (OwnBase(true) + kGroups * kOwn * OwnSlot(true)) > (OwnBase(false) + kGroups * kOwn * OwnSlot(false))
+        ? (OwnBase(true) + kGroups * kOwn * OwnSlot(true))
+        : (OwnBase(false) + kGroups * kOwn * OwnSlot(false));
+constexpr uint32_t kStagingOff = kRegionOff + kRegion;
 constexpr size_t kTcSmem = kStagingOff + kStaging + 1024;
 
 // Stage description handed from the loaders to the MMA thread.
@@ -95,8 +102,8 @@ struct Sync {
     uint64_t accFull[kAccs], accEmpty[kAccs];
     uint64_t rawFull[kRaw], rawEmpty[kRaw];
     StageHdr hdr[kPlaneSets];
-    int rawInfo[kRaw];      // stage place, packed (see InfoSt); written and read by the first converter
-    int rawK[kRaw][2];      // stage's first K index and the tile's K end
+    int ownInfo[kGroups][kOwn];  // stage place, packed (see InfoSt); written and read by a group's first thread
+    int rawK[kRaw][2];           // stage's first K index and the tile's K end
     uint32_t tmem;
     int abort;
     int isLast;
@@ -149,6 +156,9 @@ __device__ __forceinline__ int InfoSt(int info) { return info & 1023; }
 __device__ __forceinline__ int InfoNst(int info) { return (info >> 10) & 1023; }
 __device__ __forceinline__ int InfoJ(int info) { return info >> 20; }
 
+// Stages between fetching the next tile's descriptor and its front.
+constexpr int kFrontLag = 2;
+
 // What the copies of one tile need.
 struct LoadMeta {
     const c32* G;
@@ -157,8 +167,8 @@ struct LoadMeta {
 };
 
 // Walks this CTA's (tile, stage) sequence.  The next tile's descriptor is
-// fetched when a tile starts and its front once the tile's first stage is
-// issued, so that neither stalls the copies.
+// fetched when a tile starts and its front a few stages later (once the
+// descriptor has arrived), so that neither load stalls the copies.
 template <bool kFwd>
 struct LoadCursor {
     const SweepFront<float>* fr;
@@ -219,7 +229,7 @@ struct LoadCursor {
     __device__ __forceinline__ void Advance() {
         ++gl;
         if (++st < m.nst) {
-            if (st == 1) PrefetchFront();
+            if (st == kFrontLag) PrefetchFront();
             return;
         }
         ti += gridDim.x;
@@ -266,7 +276,7 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
             umma::MbarArriveExpectTx(&S.rawFull[slot], bytes);
         }
         __syncwarp();
-        unsigned char* dst = raw + slot * kRawSlot;
+        unsigned char* dst = raw + slot * kRawA;
         if (bytes) {
             if (kFwd) {
                 const int rows2 = (min(kTcRows, m.rows - m.row0) + 1) & ~1;
@@ -294,35 +304,44 @@ __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
     umma::SplitTf32(x.im, hi.y, lo.y);
 }
 
-// Issues this converter thread's own copies of the cursor's stage (its B
-// entry; backward also its four 16-byte A chunks, zero-filled outside the
-// tile), commits one copy group and advances the cursor.
+// Issues this converter thread's own copies of the cursor's stage (its two
+// B entries; backward also its eight 16-byte A chunks, zero-filled outside
+// the tile), commits one copy group and moves the cursor to the group's
+// next stage.
 template <bool kFwd>
-__device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* raw, Sync& S) {
+__device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* own, int gr, Sync& S) {
     if (cur.total >= 0) {
         umma::CpAsyncCommit();
         return;
     }
-    const int slot = cur.gl % kRaw;
+    const int slot = (cur.gl / kGroups) % kOwn;
     const LoadMeta& m = cur.m;
-    const int lt = threadIdx.x - kLoad0;
-    if (lt == 0) S.rawInfo[slot] = cur.Info();  // read back by this thread for the stage header
-    const int kc = lt / kSweepCols, nn = lt % kSweepCols;
-    const int kk = cur.KBase() + kc;
-    const bool ok = kk < m.ke && nn < min(kSweepCols, cur.k - m.col0);
-    c32* rb = reinterpret_cast<c32*>(raw + slot * kRawSlot + kRawA);
-    if (kFwd) {
-        const c32* src = m.B + (int64_t)kk * 3 * cur.k + m.col0 + nn;
+    const int ct = (threadIdx.x - kLoad0) % kGroupThreads;
+    if (ct == 0) S.ownInfo[gr][slot] = cur.Info();
+    unsigned char* base = own + slot * OwnSlot(kFwd);
+    c32* rb = reinterpret_cast<c32*>(base + (kFwd ? 0 : kRawA));
+    const int ncol = min(kSweepCols, cur.k - m.col0);
+    const int kBase = cur.KBase();
 #pragma unroll
-        for (int p = 0; p < 3; ++p)
-            umma::CpAsync8(rb + p * kStageK * kSweepCols + lt, ok ? src + p * cur.k : m.B, ok ? 8u : 0u);
-    } else {
-        umma::CpAsync8(rb + lt, ok ? m.B + (int64_t)kk * cur.k + m.col0 + nn : m.B, ok ? 8u : 0u);
-        c32* ra = reinterpret_cast<c32*>(raw + slot * kRawSlot);
-        const int kBase = cur.KBase();
+    for (int j = 0; j < kStageK * kSweepCols / kGroupThreads; ++j) {
+        const int e = ct + j * kGroupThreads;
+        const int kc = e / kSweepCols, nn = e % kSweepCols;
+        const int kk = kBase + kc;
+        const bool ok = kk < m.ke && nn < ncol;
+        if (kFwd) {
+            const c32* src = m.B + (int64_t)kk * 3 * cur.k + m.col0 + nn;
 #pragma unroll
-        for (int i = 0; i < kAChunks; ++i) {
-            const int c = lt + i * kLoadThreads;
+            for (int p = 0; p < 3; ++p)
+                umma::CpAsync8(rb + p * kStageK * kSweepCols + e, ok ? src + p * cur.k : m.B, ok ? 8u : 0u);
+        } else {
+            umma::CpAsync8(rb + e, ok ? m.B + (int64_t)kk * cur.k + m.col0 + nn : m.B, ok ? 8u : 0u);
+        }
+    }
+    if (!kFwd) {
+        c32* ra = reinterpret_cast<c32*>(base);
+#pragma unroll
+        for (int i = 0; i < kStageK * kTcRows / 2 / kGroupThreads; ++i) {
+            const int c = ct + i * kGroupThreads;
             const int mm = c / (kStageK / 2), q = c % (kStageK / 2);
             const int rr = m.row0 + mm, kk0 = kBase + 2 * q;
             const int nv = (rr < m.rows) ? max(0, min(2, m.ke - kk0)) : 0;
@@ -330,23 +349,23 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* r
         }
     }
     umma::CpAsyncCommit();
-    cur.Advance();
+#pragma unroll
+    for (int i = 0; i < kGroups; ++i) cur.Advance();
 }
 
-// Converts one raw stage into plane set P; K-columns at or beyond kEnd
-// (relative to the stage's first column kBase) are taken as zero.
+// Converts one raw stage into plane set P (thread ct of a group); forward
+// K-columns at or beyond kValid are taken as zero.
 template <bool kFwd>
-__device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawSlot, int kValid) {
-    const int lt = threadIdx.x - kLoad0;
-    const c32* ra = reinterpret_cast<const c32*>(rawSlot);
+__device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawA, const unsigned char* own,
+                                             int kValid, int ct) {
     unsigned char* aHi = P;
     unsigned char* aLo = P + kAPlane;
     const c32 zero = mk<float>(0, 0);
     if (kFwd) {
-        const int row = lt % kTcRows, half = lt / kTcRows;
+        const c32* ra = reinterpret_cast<const c32*>(rawA);
+        const int row = ct;
 #pragma unroll
-        for (int i = 0; i < kAPerThread / 2; ++i) {  // chunk: complex K 2q, 2q+1
-            const int q = half * (kAPerThread / 2) + i;
+        for (int q = 0; q < kStageK / 2; ++q) {  // chunk: complex K 2q, 2q+1
             float2 h0, l0, h1, l1;
             Split2(2 * q < kValid ? ra[(2 * q) * kTcRows + row] : zero, h0, l0);
             Split2(2 * q + 1 < kValid ? ra[(2 * q + 1) * kTcRows + row] : zero, h1, l1);
@@ -356,9 +375,10 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
         }
     } else {
         // this thread's own chunks (already zero-filled outside the tile)
+        const c32* ra = reinterpret_cast<const c32*>(own);
 #pragma unroll
-        for (int i = 0; i < kAChunks; ++i) {
-            const int c = lt + i * kLoadThreads;
+        for (int i = 0; i < kStageK * kTcRows / 2 / kGroupThreads; ++i) {
+            const int c = ct + i * kGroupThreads;
             const int m = c / (kStageK / 2), q = c % (kStageK / 2);
             float2 h0, l0, h1, l1;
             Split2(ra[m * kStageK + 2 * q], h0, l0);
@@ -369,37 +389,43 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
         }
     }
     // B: entry (kc, n) becomes rows 2n, 2n+1 of B' at K positions 2kc, 2kc+1
-    const int kc = lt / kSweepCols, nn = lt % kSweepCols;
-    const c32* rb = reinterpret_cast<const c32*>(rawSlot + kRawA) + lt;
-    const c32 b = kFwd ? rb[0] + rb[kStageK * kSweepCols] + rb[2 * kStageK * kSweepCols] : rb[0];
-    float2 h, l;
-    Split2(b, h, l);
+    const c32* rb = reinterpret_cast<const c32*>(own + (kFwd ? 0 : kRawA));
     unsigned char* bHi = P + 2 * kAPlane;
     unsigned char* bLo = bHi + kBPlane;
-    const uint32_t o0 = umma::Sw128Offset(2 * nn, kc >> 1) + (kc & 1) * 8;
-    const uint32_t o1 = umma::Sw128Offset(2 * nn + 1, kc >> 1) + (kc & 1) * 8;
-    *reinterpret_cast<float2*>(bHi + o0) = make_float2(h.x, -h.y);
-    *reinterpret_cast<float2*>(bHi + o1) = make_float2(h.y, h.x);
-    *reinterpret_cast<float2*>(bLo + o0) = make_float2(l.x, -l.y);
-    *reinterpret_cast<float2*>(bLo + o1) = make_float2(l.y, l.x);
+#pragma unroll
+    for (int j = 0; j < kStageK * kSweepCols / kGroupThreads; ++j) {
+        const int e = ct + j * kGroupThreads;
+        const int kc = e / kSweepCols, nn = e % kSweepCols;
+        const c32 b = kFwd ? rb[e] + rb[kStageK * kSweepCols + e] + rb[2 * kStageK * kSweepCols + e] : rb[e];
+        float2 h, l;
+        Split2(b, h, l);
+        const uint32_t o0 = umma::Sw128Offset(2 * nn, kc >> 1) + (kc & 1) * 8;
+        const uint32_t o1 = umma::Sw128Offset(2 * nn + 1, kc >> 1) + (kc & 1) * 8;
+        *reinterpret_cast<float2*>(bHi + o0) = make_float2(h.x, -h.y);
+        *reinterpret_cast<float2*>(bHi + o1) = make_float2(h.y, h.x);
+        *reinterpret_cast<float2*>(bLo + o0) = make_float2(l.x, -l.y);
+        *reinterpret_cast<float2*>(bLo + o1) = make_float2(l.y, l.x);
+    }
 }
 
-// Converts stage g (or ends the stream); false when the role is done.
+// Converts stage g (a stage of this thread's group, plane set g % 2) or
+// ends the stream; false when the role is done.
 template <bool kFwd>
-__device__ __forceinline__ bool ConverterStep(unsigned char* smem, const LoadCursor<kFwd>& cur, int g, Sync& S,
-                                              int* status) {
-    const int ps = g % kPlaneSets, slot = g % kRaw;
+__device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char* own, const LoadCursor<kFwd>& cur,
+                                              int g, int gr, int ct, Sync& S, int* status) {
+    const int ps = gr, slot = g % kRaw, oslot = (g / kGroups) % kOwn;
     const bool valid = cur.Valid(g);
     if (kFwd && valid && !Wait(&S.rawFull[slot], (g / kRaw) & 1, S, status)) return false;
-    if (g >= kPlaneSets && !Wait(&S.planeEmpty[ps], ((g / kPlaneSets) - 1) & 1, S, status)) return false;
-    umma::CpAsyncWait<kAhead>();  // this thread's own copies of stage g have landed
+    if (g >= kGroups && !Wait(&S.planeEmpty[ps], ((g / kGroups) - 1) & 1, S, status)) return false;
+    umma::CpAsyncWait<kAheadOwn>();  // this thread's own copies of stage g have landed
     if (valid) {
         const int kValid = kFwd ? S.rawK[slot][1] - S.rawK[slot][0] : kStageK;
-        ConvertStage<kFwd>(smem + ps * kPlaneSet, smem + kRawOff + slot * kRawSlot, kValid);
+        ConvertStage<kFwd>(smem + ps * kPlaneSet, smem + kRegionOff + slot * kRawA, own + oslot * OwnSlot(kFwd),
+                           kValid, ct);
     }
     umma::FenceProxyAsync();
-    if (threadIdx.x == kLoad0) {
-        const int info = S.rawInfo[slot];
+    if (ct == 0) {
+        const int info = S.ownInfo[gr][oslot];
         S.hdr[ps] = valid ? StageHdr{1, InfoSt(info), InfoNst(info), InfoJ(info)} : StageHdr{0, 0, 0, 0};
     }
     umma::MbarArrive(&S.planeFull[ps]);
@@ -410,14 +436,17 @@ __device__ __forceinline__ bool ConverterStep(unsigned char* smem, const LoadCur
 template <bool kFwd>
 __device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
                               int k, unsigned char* smem, Sync& S, int* status) {
+    const int lt = threadIdx.x - kLoad0;
+    const int gr = lt / kGroupThreads, ct = lt % kGroupThreads;
+    unsigned char* own = smem + kRegionOff + OwnBase(kFwd) + gr * kOwn * OwnSlot(kFwd);
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
-    unsigned char* raw = smem + kRawOff;
+    for (int i = 0; i < gr; ++i) cur.Advance();
 #pragma unroll
-    for (int a = 0; a < kAhead; ++a) IssueOwn(cur, raw, S);
-    for (int g = 0;; ++g) {
-        IssueOwn(cur, raw, S);
-        if (!ConverterStep<kFwd>(smem, cur, g, S, status)) break;
+    for (int a = 0; a < kAheadOwn; ++a) IssueOwn(cur, own, gr, S);
+    for (int g = gr;; g += kGroups) {
+        IssueOwn(cur, own, gr, S);
+        if (!ConverterStep<kFwd>(smem, own, cur, g, gr, ct, S, status)) break;
     }
     umma::CpAsyncWaitAll();
 }
@@ -621,7 +650,7 @@ __device__ void EpilogueRole(const SweepFront<float>* __restrict__ fr, const Swe
 __device__ __forceinline__ void InitSync(Sync& S) {
     if (threadIdx.x == 0) {
         for (int i = 0; i < kPlaneSets; ++i) {
-            umma::MbarInit(&S.planeFull[i], kLoadThreads);
+            umma::MbarInit(&S.planeFull[i], kGroupThreads);
             umma::MbarInit(&S.planeEmpty[i], 1);
         }
         for (int i = 0; i < kAccs; ++i) {
@@ -630,7 +659,7 @@ __device__ __forceinline__ void InitSync(Sync& S) {
         }
         for (int i = 0; i < kRaw; ++i) {
             umma::MbarInit(&S.rawFull[i], 1);
-            umma::MbarInit(&S.rawEmpty[i], kLoadThreads);
+            umma::MbarInit(&S.rawEmpty[i], kGroupThreads);
         }
         S.abort = 0;
         umma::FenceMbarInit();
@@ -669,7 +698,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
     } else if (tid == kMma0) {
         MmaRole<true>(smem, S, work.status);
     } else if (tid >= kProd0) {
-        ProducerRole<true>(fr, tiles, n, k, smem + kRawOff, S, work.status);
+        ProducerRole<true>(fr, tiles, n, k, smem + kRegionOff, S, work.status);
     }
     Teardown(S);
 }
