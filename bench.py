@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradients/s arm")
+    ap.add_argument("--grad-config", default="layered_faults_96")
     ap.add_argument("--sweep-probe", action="store_true",
                     help="profiling driver: Initialize (mixed) + two sweeps on the device, then exit")
     return ap.parse_args()
@@ -198,6 +200,46 @@ def run_arm(H, w, vel_d, rhs_d, X, precision, steps, warmup, ws, stream, clocks=
     solve_ms = max_over_ranks(solve_ms, ws)
     setup_ms = max_over_ranks(setup_ms, ws)
     return dict(total_ms=total_ms, setup_ms=setup_ms, solve_ms=solve_ms, stats=stats)
+
+
+def gradient_arm(args, ws, local):
+    """Gradients/s: each step is one full misfit gradient of a velocity model
+    -- Initialize (mixed), forward solve of every source, adjoint solve with
+    the same factors and the device gradient kernel -- through the torch
+    autograd layer (psp_b200.autograd)."""
+    import torch
+    import psp_b200 as P
+    from psp_b200.autograd import misfit_and_gradient
+    w = workload(args.grad_config)
+    N = w.disc.nx * w.disc.ny * w.disc.nz
+    k = w.k
+    H = P.DistHelmholtz(w.disc, device=local)
+    vel = torch.from_numpy(w.velocity.reshape(-1)).cuda()
+    f = torch.from_numpy(np.ascontiguousarray(w.rhs.reshape(N, k))).cuda()
+    recv = torch.from_numpy(w.meta["receivers"]).cuda()
+    H.Initialize(torch.from_numpy(w.meta["observed_model"].reshape(-1)).cuda(), precision=P.FP64)
+    u_obs = f.clone()
+    H.Solve(u_obs, RESTART, REL_TOL)
+    data = u_obs[recv].clone()
+    del u_obs
+    for _ in range(args.warmup):
+        J, g = misfit_and_gradient(H, vel, f, recv, data, RESTART, REL_TOL, P.MIXED)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        J, g = misfit_and_gradient(H, vel, f, recv, data, RESTART, REL_TOL, P.MIXED)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    out = {"value": ws * args.steps / (ms * 1e-3), "unit": "gradients/s", "ms_per_gradient": ms / args.steps,
+           "workload": args.grad_config, "grid": [w.disc.nx, w.disc.ny, w.disc.nz], "sources": k,
+           "receivers": int(len(w.meta["receivers"])), "precision": "mixed",
+           "step": "Initialize + forward solve + adjoint solve + gradient kernel",
+           "misfit": float(J), "gradient_norm": float(torch.linalg.norm(g))}
+    H.Finalize()
+    return out
 
 
 class _Null:
@@ -361,6 +403,11 @@ def main():
         e2e = {"value": ws * k * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(N * 8 + N * k * 16), "d2h_bytes_per_step": int(N * k * 16)}
 
+    grad = None
+    if not args.no_grad:
+        H.Finalize()
+        grad = gradient_arm(args, ws, local)
+
     prof = profile_step(H, vel_d, rhs_d, X, P.MIXED, stream)
     roof = roofline_from_profile(prof, peaks)
     launches_per_step = sum(v["launches"] for n, v in prof.items() if n != "sweep")
@@ -393,6 +440,7 @@ def main():
             "fp64": fp64,
             "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
             "e2e": e2e,
+            "gradients_per_s": grad,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -119,6 +119,18 @@ int psp_cu_precondition_device(psp_cu_handle* h, double* d_B, int k);
  * handle. */
 int psp_cu_multiply_device_noalloc(psp_cu_handle* h, double* d_B, int k);
 
+/* Velocity gradient of a real misfit J(u(vel)), u = A(vel)^{-1} f:
+ * d_grad[i] (+)= -Re( dA_ii/dvel_i * sum_r d_Z[i,r] d_U[i,r] ) over device
+ * natural-order grids of k right-hand sides, where d_U holds the forward
+ * fields and d_Z the adjoint fields A d_Z = conj(dJ/dconj(u)) (a solve with
+ * the same factors, the operator being complex symmetric).  No counterpart
+ * in the reference, which has no adjoint; dA_ii/dvel_i = 2 omega^2/vel_i^3 *
+ * s1 s2 s3 differentiates FormGlobalRow's centre term
+ * (initialize_finalize.hpp:567-568).  d_grad holds nx*ny*nz doubles;
+ * accumulate != 0 adds to it.  Requires an initialized handle. */
+int psp_cu_gradient_device(psp_cu_handle* h, const double* d_U, const double* d_Z, int k, double* d_grad,
+                           int accumulate);
+
 /* B := T_p B on panel p only (SolvePanel, solve.hpp:736-882); host grid. */
 int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel);
 

@@ -71,7 +71,7 @@ C_ABI_SYMBOLS = [
     "psp_cu_multiply_device", "psp_cu_precondition_device", "psp_cu_solve_panel", "psp_cu_set_max_iterations",
     "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class", "psp_cu_get_stream",
     "psp_cu_set_profiling", "psp_cu_profile_reset", "psp_cu_profile_get", "psp_cu_sweep_cost",
-    "psp_cu_multiply_device_noalloc",
+    "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -115,6 +115,7 @@ def lib():
         L.psp_cu_profile_get.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp]
         L.psp_cu_sweep_cost.argtypes = [vp, ctypes.c_int, dp, dp]
         L.psp_cu_multiply_device_noalloc.argtypes = [vp, vp, ctypes.c_int]
+        L.psp_cu_gradient_device.argtypes = [vp, vp, vp, ctypes.c_int, vp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -278,11 +279,13 @@ class DistHelmholtz:
                 raise LogicError("Velocity grid is incorrect")
             v = velocity.contiguous()
             _check(lib().psp_cu_initialize_device(self._h, ctypes.c_void_p(v.data_ptr()), panelScheme, precision))
+            self.factor_version = getattr(self, "factor_version", 0) + 1
             return
         v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
         if v.size != self.N:
             raise LogicError("Velocity grid is incorrect")
         _check(lib().psp_cu_initialize(self._h, _dptr(v), panelScheme, precision))
+        self.factor_version = getattr(self, "factor_version", 0) + 1
 
     def Solve(self, B, m=20, relTol=1e-4, viewIterates=False):
         """Solve in place (solve.hpp:12-56).  ``B`` is a complex DistUniformGrid
@@ -379,6 +382,23 @@ class DistHelmholtz:
 
     def precondition_device(self, B):
         _check(lib().psp_cu_precondition_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+
+    def gradient_device(self, U, Z, grad=None, accumulate=False):
+        """Velocity gradient -Re(dA_ii/dvel_i * sum_r Z[i,r] U[i,r]) of a real
+        misfit from forward fields U and adjoint fields Z (CUDA complex128
+        tensors of nx*ny*nz*k entries, natural order); returns (or adds to)
+        a CUDA float64 tensor of nx*ny*nz entries."""
+        import torch
+        k = U.numel() // self.N
+        if U.numel() != Z.numel() or k * self.N != U.numel():
+            raise LogicError("U and Z must be grids of the same k right-hand sides")
+        if grad is None:
+            grad = torch.zeros(self.N, dtype=torch.float64, device=U.device)
+            accumulate = False
+        U, Z = U.contiguous(), Z.contiguous()
+        _check(lib().psp_cu_gradient_device(self._h, ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(Z.data_ptr()), k,
+                                            ctypes.c_void_p(grad.data_ptr()), 1 if accumulate else 0))
+        return grad
 
 
 def _stats_dict(st):

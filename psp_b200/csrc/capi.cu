@@ -163,6 +163,15 @@ int psp_cu_precondition_device(psp_cu_handle* h, double* d_B, int k) {
     return Guard([&] { h->solver->PreconditionDevice(reinterpret_cast<psp_b200::z64*>(d_B), k); });
 }
 
+int psp_cu_gradient_device(psp_cu_handle* h, const double* d_U, const double* d_Z, int k, double* d_grad,
+                           int accumulate) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        h->solver->GradientDevice(reinterpret_cast<const psp_b200::z64*>(d_U),
+                                  reinterpret_cast<const psp_b200::z64*>(d_Z), k, d_grad, accumulate != 0);
+    });
+}
+
 int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {

@@ -79,6 +79,26 @@ __global__ void __launch_bounds__(kThreads) helmholtz_apply_kernel(const z64* __
     }
 }
 
+// ---------------------------------------------------------------- velocity gradient
+
+__global__ void __launch_bounds__(kThreads) velocity_gradient_kernel(const z64* __restrict__ U,
+                                                                     const z64* __restrict__ Z,
+                                                                     const double* __restrict__ vel, StencilParams sp,
+                                                                     int k, double* __restrict__ grad, int accumulate) {
+    const int64_t nxy = (int64_t)sp.nx * sp.ny, n = nxy * sp.nz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int xx = (int)(i % sp.nx), yy = (int)((i / sp.nx) % sp.ny), zz = (int)(i / nxy);
+        const int v = sp.nz - 1 - zz;
+        const double a = vel[i];
+        const z64 s = sp.s1[xx + 1] * sp.s2[yy + 1] * sp.s3[v + 1];
+        const z64 dA = (2.0 * sp.omega * sp.omega / (a * a * a)) * s;
+        z64 acc = mk(0.0, 0.0);
+        for (int r = 0; r < k; ++r) cfma(acc, Z[i * k + r], U[i * k + r]);
+        const double g = -(dA * acc).re;
+        grad[i] = accumulate ? grad[i] + g : g;
+    }
+}
+
 // ---------------------------------------------------------------- batched GEMM
 
 template <typename R, int BM, int BN, int BK, int TM, int TN>
@@ -420,6 +440,13 @@ void LaunchHelmholtzApply(const z64* x, z64* y, const z64* b, const double* vel,
                           cudaStream_t st) {
     dim3 grid(CeilDiv(sp.nx, kApplyTX), sp.ny, sp.nz);
     helmholtz_apply_kernel<<<grid, kThreads, 0, st>>>(x, y, b, vel, sp, k);
+    CUDA_LAUNCH_CHECK();
+}
+
+void LaunchVelocityGradient(const z64* U, const z64* Z, const double* vel, const StencilParams& sp, int k,
+                            double* grad, int accumulate, cudaStream_t st) {
+    const int64_t n = (int64_t)sp.nx * sp.ny * sp.nz;
+    velocity_gradient_kernel<<<ElementwiseGrid(n), kThreads, 0, st>>>(U, Z, vel, sp, k, grad, accumulate);
     CUDA_LAUNCH_CHECK();
 }
 

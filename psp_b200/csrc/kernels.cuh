@@ -28,6 +28,15 @@ struct StencilParams {
 void LaunchHelmholtzApply(const z64* x, z64* y, const z64* b, const double* vel, const StencilParams& sp, int k,
                           cudaStream_t st);
 
+// grad[i] (+)= -Re( dA_ii/dvel_i * sum_r Z[i,r] U[i,r] ) for natural-order
+// [N][k] grids: the velocity gradient of a real misfit whose forward fields
+// are U and whose adjoint fields (A Z = conj of the misfit's field gradient)
+// are Z.  dA_ii/dvel_i = 2 omega^2 / vel_i^3 * s1 s2 s3 differentiates the
+// centre term of FormGlobalRow (initialize_finalize.hpp:567-568); the
+// operator is complex symmetric, so Z reuses the forward factors.
+void LaunchVelocityGradient(const z64* U, const z64* Z, const double* vel, const StencilParams& sp, int k,
+                            double* grad, int accumulate, cudaStream_t st);
+
 // ------------------------------------------------------------------ batched GEMM
 
 // C = alpha * op(A) * diag(d) * op(B) + beta * C, complex, no conjugation.

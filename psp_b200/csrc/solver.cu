@@ -988,6 +988,14 @@ void Helmholtz::MultiplyDevice(z64* B, int k) {
     CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 
+void Helmholtz::GradientDevice(const z64* U, const z64* Z, int k, double* grad, bool accumulate) {
+    if (!dVel_.p) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    if (k <= 0) throw PspError(kLogicError, "number of right-hand sides must be positive");
+    CUDA_CHECK(cudaSetDevice(device_));
+    LaunchVelocityGradient(U, Z, dVel_.as<double>(), sp_, k, grad, accumulate ? 1 : 0, stream_);
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
 void Helmholtz::EnsureWorkspace(int k, int m) {
     if (wsK_ == k && wsM_ == m) return;
     const int64_t nk = NumUnknowns() * k;

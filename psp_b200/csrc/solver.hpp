@@ -84,6 +84,9 @@ public:
     void MultiplyDevice(z64* B, int k);
     void PreconditionDevice(z64* B, int k);
     void SolvePanelDevice(z64* B, int k, int panel);
+    // grad (+)= velocity gradient from forward fields U and adjoint fields Z
+    // (device natural-order [N][k] grids; grad is a device array of N reals).
+    void GradientDevice(const z64* U, const z64* Z, int k, double* grad, bool accumulate);
 
     const Analysis& analysis() const { return an_; }
     int64_t NumUnknowns() const { return (int64_t)an_.disc.nx * an_.disc.ny * an_.disc.nz; }

@@ -134,9 +134,69 @@ def small_case(interior=(12, 13, 14), pml=5, freq=2.0, k=3, seed=7, top_pml=True
                     dict(x0=x0.tolist(), sources=centres, freq=freq))
 
 
+def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, ppw=10.0, perturb=0.03):
+    """Differentiation case: 8 layers of 1.5-5.5 (km/s) whose interface
+    depths jitter by +-15 % of the layer thickness, offset across two dipping
+    planar faults; uniform spacing h = 1/(max interior + 1) (km), and omega
+    chosen so the slowest layer has ``ppw`` points per wavelength; k point
+    sources (Gaussians of width 2h) on the first plane below the top PML and
+    receivers at every interior point of that plane.  ``meta`` holds the
+    receiver indices (natural order) and the model the observed data come
+    from (velocity perturbed by +-3 % with a seeded smooth pattern)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = [m + 2 * pml for m in interior]
+    h = 1.0 / (max(interior) + 1)
+    X, Y, Z = [(np.arange(nn) - pml + 1) * h for nn in n]
+    Zc, Yc, Xc = np.meshgrid(Z, Y, X, indexing="ij")
+    depth = Z[-1] - Z[0]
+    speeds = np.linspace(1.5, 5.5, n_layers)
+    thick = depth / n_layers
+    tops = np.array([Z[0] + thick * (i + rng.uniform(-0.15, 0.15)) for i in range(1, n_layers)])
+    shift = np.zeros_like(Zc)
+    faults = []
+    for _ in range(2):
+        normal = np.array([rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(0.3, 0.8)])
+        normal /= np.linalg.norm(normal)
+        point = np.array([rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7), 0.5 * depth + Z[0]])
+        throw = rng.uniform(0.5, 1.0) * 0.3 * thick
+        side = (Xc - point[0]) * normal[0] + (Yc - point[1]) * normal[1] + (Zc - point[2]) * normal[2] > 0
+        shift = shift + np.where(side, throw, 0.0)
+        faults.append((normal.tolist(), point.tolist(), float(throw)))
+    # the solver's z index 0 is the top face (sweep coordinate v = nz-1-z), so
+    # depth grows with z and the slow layer sits at the surface
+    layer = np.searchsorted(tops, Zc - shift)
+    vel = np.ascontiguousarray(speeds[np.clip(layer, 0, n_layers - 1)])
+    omega = 2 * math.pi * speeds[0] / (ppw * h)
+    w = [(nn + 1) * h for nn in n]
+    disc = Discretization(omega, n[0], n[1], n[2], w[0], w[1], w[2], bcs=(PML,) * 5, pml=(pml,) * 3, sigma=SIGMA)
+    # sources and receivers on the first plane below the top PML (solver z index pml)
+    zs = pml
+    sig = 2.0 * h
+    rhs = np.zeros((n[2], n[1], n[0], k), dtype=np.complex128)
+    centres = []
+    for r in range(k):
+        ix = rng.integers(pml + 2, n[0] - pml - 2)
+        iy = rng.integers(pml + 2, n[1] - pml - 2)
+        centres.append((int(ix), int(iy), zs))
+        gx = np.exp(-((X - X[ix]) ** 2) / (2 * sig ** 2))
+        gy = np.exp(-((Y - Y[iy]) ** 2) / (2 * sig ** 2))
+        gz = np.exp(-((np.arange(n[2]) - zs) * h) ** 2 / (2 * sig ** 2))
+        rhs[..., r] = -(gz[:, None, None] * gy[None, :, None] * gx[None, None, :])
+    yy, xx = np.meshgrid(np.arange(pml, n[1] - pml), np.arange(pml, n[0] - pml), indexing="ij")
+    receivers = (xx + yy * n[0] + zs * n[0] * n[1]).reshape(-1)
+    pattern = np.sin(3.1 * Xc / Xc.max() + 1.7) * np.cos(2.3 * Yc / Yc.max()) * np.sin(4.1 * Zc / Zc.max() + 0.4)
+    observed_model = np.ascontiguousarray(vel * (1.0 + perturb * pattern))
+    return Workload("layered_faults", disc, vel, rhs, pml, interior,
+                    dict(receivers=receivers, observed_model=observed_model, faults=faults, h=h,
+                         omega=omega, sources=centres, layer_tops=tops.tolist()))
+
+
 CONFIGS = {
     "plain_bump_50": plain_bump,
     "smooth_anomalies_116": smooth_anomalies,
     # profiling-sized member of the same family (factors ~0.5 GB, above L2)
     "smooth_anomalies_56": lambda: smooth_anomalies(interior=(40, 40, 40), pml=8, freq=4.0, k=16),
+    "layered_faults_96": layered_faults,
+    # test-sized member of the same family
+    "layered_faults_24": lambda: layered_faults(interior=(20, 20, 16), pml=5, k=4, ppw=12.0),
 }

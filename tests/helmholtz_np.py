@@ -105,3 +105,32 @@ def apply_panel_inverse(d, vel, B, low_v, depth, padding, damping):
     out = Bv.copy()
     out[low_v:low_v + depth] = X[padding * nxy:].reshape(depth, nxy, k)
     return out[::-1].reshape(B.shape)
+
+
+def velocity_derivative_diag(d, vel):
+    """dA_ii/dvel_i in natural z-major order: the derivative of FormGlobalRow's
+    centre term -(omega/vel)^2 s1 s2 s3 (initialize_finalize.hpp:567-568),
+    i.e. 2 omega^2 / vel^3 * s1 s2 s3.  ``vel`` has shape (nz, ny, nx)."""
+    hx, hy, hz, s1, s2 = _tables(d)
+    s3 = lambda v: stretch(v, d.nz, d.bz, d.sigmaz, hz, d.omega, True, d.topBC == PML)
+    t1 = np.array([s1(x) for x in range(d.nx)])
+    t2 = np.array([s2(y) for y in range(d.ny)])
+    t3 = np.array([s3(d.nz - 1 - z) for z in range(d.nz)])
+    s = t3[:, None, None] * t2[None, :, None] * t1[None, None, :]
+    return (2 * d.omega ** 2 / np.asarray(vel) ** 3 * s).reshape(-1)
+
+
+def adjoint_gradient(d, vel, f, receivers, data):
+    """Misfit J = 1/2 sum |u[receivers] - data|^2 with u = A(vel)^{-1} f by a
+    sparse direct solve, and its velocity gradient by the adjoint-state
+    method (A is complex symmetric, so the adjoint solve reuses A)."""
+    import scipy.sparse.linalg as spla
+    lu = spla.splu(global_matrix(d, vel).tocsc())
+    u = lu.solve(np.ascontiguousarray(f))
+    r = u[receivers] - data
+    J = 0.5 * float(np.sum(np.abs(r) ** 2))
+    G = np.zeros_like(u)
+    G[receivers] = r
+    z = lu.solve(np.conj(G))
+    g = -np.real(velocity_derivative_diag(d, vel) * np.sum(z * u, axis=1))
+    return J, g, u

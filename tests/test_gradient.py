@@ -1,0 +1,94 @@
+"""Velocity gradients by the adjoint-state method (the differentiation layer;
+the reference has no adjoint).
+
+CPU: the adjoint formula against central finite differences of the misfit,
+both from sparse direct solves of the independent numpy operator.  GPU: the
+device gradient kernel against the same formula, and the autograd path
+(forward solve, adjoint solve with the forward factors, gradient kernel)
+against the direct-solve adjoint gradient.
+"""
+import numpy as np
+import pytest
+
+import helmholtz_np as hn
+from psp_b200 import workloads as W
+
+
+def _misfit_case():
+    w = W.small_case()
+    d = w.disc
+    vel = np.asarray(w.velocity).reshape(d.nz, d.ny, d.nx)
+    rng = np.random.Generator(np.random.PCG64(2024))
+    N = d.nx * d.ny * d.nz
+    receivers = np.sort(rng.choice(N, size=200, replace=False))
+    # observed data from a 3 % perturbed model
+    pert = vel * (1 + 0.03 * np.sin(np.linspace(0, 6, vel.size)).reshape(vel.shape))
+    import scipy.sparse.linalg as spla
+    f = np.ascontiguousarray(np.asarray(w.rhs).reshape(N, -1))
+    u_obs = spla.splu(hn.global_matrix(d, pert).tocsc()).solve(f)
+    return w, d, vel, f, receivers, u_obs[receivers]
+
+
+def test_adjoint_formula_matches_finite_differences():
+    w, d, vel, f, receivers, data = _misfit_case()
+    J0, g, _ = hn.adjoint_gradient(d, vel, f, receivers, data)
+    assert J0 > 0
+    rng = np.random.Generator(np.random.PCG64(5))
+    voxels = rng.choice(vel.size, size=6, replace=False)
+    for i in voxels:
+        h = 1e-4 * vel.reshape(-1)[i]
+        vp, vm = vel.copy().reshape(-1), vel.copy().reshape(-1)
+        vp[i] += h
+        vm[i] -= h
+        Jp = hn.adjoint_gradient(d, vp.reshape(vel.shape), f, receivers, data)[0]
+        Jm = hn.adjoint_gradient(d, vm.reshape(vel.shape), f, receivers, data)[0]
+        fd = (Jp - Jm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-5 * max(abs(g[i]), 1e-3 * np.abs(g).max()), (i, fd, g[i])
+
+
+@pytest.mark.gpu
+def test_gradient_kernel_matches_formula(product_lib):
+    import torch
+    import psp_b200 as P
+    w = W.small_case()
+    d = w.disc
+    H = P.DistHelmholtz(d)
+    H.Initialize(w.velocity, precision=P.FP64)
+    rng = np.random.Generator(np.random.PCG64(11))
+    N, k = d.nx * d.ny * d.nz, 3
+    U = rng.standard_normal((N, k)) + 1j * rng.standard_normal((N, k))
+    Z = rng.standard_normal((N, k)) + 1j * rng.standard_normal((N, k))
+    g = H.gradient_device(torch.from_numpy(U).cuda(), torch.from_numpy(Z).cuda()).cpu().numpy()
+    vel = np.asarray(w.velocity).reshape(d.nz, d.ny, d.nx)
+    ref = -np.real(hn.velocity_derivative_diag(d, vel) * np.sum(Z * U, axis=1))
+    assert np.linalg.norm(g - ref) <= 1e-12 * np.linalg.norm(ref)
+    g2 = H.gradient_device(torch.from_numpy(U).cuda(), torch.from_numpy(Z).cuda(),
+                           grad=torch.from_numpy(ref.copy()).cuda(), accumulate=True).cpu().numpy()
+    assert np.linalg.norm(g2 - 2 * ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [(0, 1e-7), (1, 2e-3)])
+def test_autograd_gradient_matches_direct_adjoint(product_lib, precision, tol):
+    import torch
+    import psp_b200 as P
+    from psp_b200.autograd import misfit_and_gradient, helmholtz_solve
+    w, d, vel, f_np, receivers, data = _misfit_case()
+    J_ref, g_ref, u_ref = hn.adjoint_gradient(d, vel, f_np, receivers, data)
+    H = P.DistHelmholtz(d)
+    v = torch.from_numpy(vel.reshape(-1).copy()).cuda()
+    f = torch.from_numpy(f_np).cuda()
+    J, g = misfit_and_gradient(H, v, f, torch.from_numpy(receivers).cuda(), torch.from_numpy(data).cuda(),
+                               m=60, rel_tol=1e-11 if precision == 0 else 1e-8, precision=precision)
+    assert abs(float(J) - J_ref) <= tol * J_ref
+    assert np.linalg.norm(g.cpu().numpy() - g_ref) <= tol * np.linalg.norm(g_ref)
+    # the source gradient: dL/dconj(f) = conj(z), z = A^{-1} conj(dL/dconj(u))
+    vv = v.clone()
+    ff = f.clone().requires_grad_(True)
+    u = helmholtz_solve(H, vv, ff, m=60, rel_tol=1e-11, precision=P.FP64)
+    (u.real.sum() + 2 * u.imag.sum()).backward()
+    import scipy.sparse.linalg as spla
+    lu = spla.splu(hn.global_matrix(d, vel).tocsc())
+    G = np.ones_like(u_ref) * (1 + 2j)  # dL/dconj(u) for L = sum(re u) + 2 sum(im u)
+    ref = np.conj(lu.solve(np.conj(G)))
+    assert np.linalg.norm(ff.grad.cpu().numpy() - ref) <= 1e-7 * np.linalg.norm(ref)
