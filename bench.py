@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradients/s arm")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch-of-48-problems arm")
     ap.add_argument("--grad-config", default="layered_faults_96")
     ap.add_argument("--sweep-probe", action="store_true",
                     help="profiling driver: Initialize (mixed) + two sweeps on the device, then exit")
@@ -137,33 +138,21 @@ class ClockSampler:
 
 
 def dist_setup(args):
-    import torch
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from psp_b200 import ranks
+    ws, rank, local = ranks.from_env()
     if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        ranks.init("nccl", 300, local)
     return ws, rank, local
 
 
 def max_over_ranks(x, ws):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from psp_b200 import ranks
+    return ranks.max_over_ranks(x, ws)
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from psp_b200 import ranks
+    ranks.barrier(ws)
 
 
 def run_arm(H, w, vel_d, rhs_d, X, precision, steps, warmup, ws, stream, clocks=None):
@@ -240,6 +229,39 @@ def gradient_arm(args, ws, local):
            "misfit": float(J), "gradient_norm": float(torch.linalg.norm(g))}
     H.Finalize()
     return out
+
+
+def batch_arm(args, ws, rank, local):
+    """Throughput over the batching workload: 48 independent problems (sides
+    32-96, k = 1-8) split over the ranks by predicted cost (longest
+    processing time first); every rank factors and solves its share
+    (mixed precision) with no communication; RHS/s = all right-hand sides /
+    the slowest rank's time.  Solutions stay on their rank (no gather)."""
+    import torch
+    import psp_b200 as P
+    from psp_b200 import batch as B
+    probs = W_batch()
+    costs = [B.predicted_cost(p.disc, p.k) for p in probs]
+    bins, loads = B.lpt_assign(costs, ws)
+    warm = probs[min(range(len(probs)), key=lambda i: costs[i])]
+    B.solve_batch([warm], precision=P.MIXED, device=local, costs=[1.0])
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, rep = B.solve_batch(probs, RESTART, REL_TOL, P.MIXED, rank, ws, local, gather=False, costs=costs)
+    torch.cuda.synchronize()
+    sec = max_over_ranks(time.perf_counter() - t0, ws)
+    total_k = sum(p.k for p in probs)
+    return {"value": total_k / sec, "unit": "RHS/s", "seconds": sec, "problems": len(probs), "rhs": total_k,
+            "workload": "batch_48", "precision": "mixed", "scaling": "strong (fixed batch over ranks)",
+            "predicted_loads_s": [round(x, 4) for x in loads],
+            "problems_per_rank": [len(b) for b in bins],
+            "timing": "host wall clock around the rank's share, max over ranks (many short solves)"}
+
+
+def W_batch():
+    from psp_b200 import workloads as W
+    return W.batch_problems()
 
 
 class _Null:
@@ -403,6 +425,11 @@ def main():
         e2e = {"value": ws * k * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(N * 8 + N * k * 16), "d2h_bytes_per_step": int(N * k * 16)}
 
+    batch = None
+    if not args.no_batch:
+        H.Finalize()
+        batch = batch_arm(args, ws, rank, local)
+
     grad = None
     if not args.no_grad:
         H.Finalize()
@@ -441,6 +468,7 @@ def main():
             "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
             "e2e": e2e,
             "gradients_per_s": grad,
+            "batch": batch,
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -85,6 +85,18 @@ int psp_cu_initialize(psp_cu_handle* h, const double* velocity, int panel_scheme
 /* Same with the velocity already in device memory of the handle's GPU. */
 int psp_cu_initialize_device(psp_cu_handle* h, const double* d_velocity, int panel_scheme, int precision);
 
+/* Batched variants over count independent problems, one handle each (the
+ * handles may live on different GPUs).  No counterpart in the reference,
+ * which runs one problem per SPMD job; each element is exactly
+ * psp_cu_initialize / psp_cu_solve on its own handle, run in order.  The
+ * first failing element stops the batch: its status is returned and its
+ * index written to *failed (-1 when every element succeeds); stats (if not
+ * NULL) holds count entries. */
+int psp_cu_initialize_batch(psp_cu_handle* const* h, const double* const* velocity, int count, int panel_scheme,
+                            int precision, int* failed);
+int psp_cu_solve_batch(psp_cu_handle* const* h, double* const* B, const int* k, int count, int m, double rel_tol,
+                       psp_cu_stats* stats, int* failed);
+
 /* DistHelmholtz::Solve(B, m, relTol) (include/psp/dist_helmholtz/solve.hpp:12-56):
  * B is a host grid of nx*ny*nz*k complex values, overwritten by the solution. */
 int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_cu_stats* stats);

@@ -71,7 +71,7 @@ C_ABI_SYMBOLS = [
     "psp_cu_multiply_device", "psp_cu_precondition_device", "psp_cu_solve_panel", "psp_cu_set_max_iterations",
     "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class", "psp_cu_get_stream",
     "psp_cu_set_profiling", "psp_cu_profile_reset", "psp_cu_profile_get", "psp_cu_sweep_cost",
-    "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device",
+    "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device", "psp_cu_initialize_batch", "psp_cu_solve_batch",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -116,6 +116,10 @@ def lib():
         L.psp_cu_sweep_cost.argtypes = [vp, ctypes.c_int, dp, dp]
         L.psp_cu_multiply_device_noalloc.argtypes = [vp, vp, ctypes.c_int]
         L.psp_cu_gradient_device.argtypes = [vp, vp, vp, ctypes.c_int, vp, ctypes.c_int]
+        L.psp_cu_initialize_batch.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(dp), ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ip]
+        L.psp_cu_solve_batch.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(dp), ip, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, ctypes.POINTER(_Stats), ip]
         _lib = L
     return _lib
 
@@ -399,6 +403,40 @@ class DistHelmholtz:
         _check(lib().psp_cu_gradient_device(self._h, ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(Z.data_ptr()), k,
                                             ctypes.c_void_p(grad.data_ptr()), 1 if accumulate else 0))
         return grad
+
+
+def initialize_batch(solvers, velocities, panelScheme=CLIQUE_LDL_SELINV_1D, precision=FP64):
+    """psp_cu_initialize_batch: factor independent problems (one DistHelmholtz
+    each, host velocities in natural order) in one call."""
+    n = len(solvers)
+    vs = [np.ascontiguousarray(v, dtype=np.float64).reshape(-1) for v in velocities]
+    for s, v in zip(solvers, vs):
+        if v.size != s.N:
+            raise LogicError("Velocity grid is incorrect")
+    hs = (ctypes.c_void_p * n)(*[s._h.value for s in solvers])
+    ps = (ctypes.POINTER(ctypes.c_double) * n)(*[_dptr(v) for v in vs])
+    failed = ctypes.c_int()
+    _check(lib().psp_cu_initialize_batch(hs, ps, n, panelScheme, precision, ctypes.byref(failed)))
+    for s in solvers:
+        s.factor_version = getattr(s, "factor_version", 0) + 1
+
+
+def solve_batch(solvers, grids, m=20, relTol=1e-4):
+    """psp_cu_solve_batch: solve in place host grids (C-contiguous complex128,
+    nx*ny*nz*k each) of independent problems; returns their stats."""
+    n = len(solvers)
+    ks = []
+    for s, g in zip(solvers, grids):
+        if g.dtype != np.complex128 or not g.flags["C_CONTIGUOUS"] or g.size % s.N:
+            raise LogicError("B must be a C-contiguous complex128 grid")
+        ks.append(g.size // s.N)
+    hs = (ctypes.c_void_p * n)(*[s._h.value for s in solvers])
+    ps = (ctypes.POINTER(ctypes.c_double) * n)(*[_dptr(g.view(np.float64)) for g in grids])
+    karr = (ctypes.c_int * n)(*ks)
+    st = (_Stats * n)()
+    failed = ctypes.c_int()
+    _check(lib().psp_cu_solve_batch(hs, ps, karr, n, m, relTol, st, ctypes.byref(failed)))
+    return [_stats_dict(st[i]) for i in range(n)]
 
 
 def _stats_dict(st):

@@ -113,6 +113,38 @@ int psp_cu_initialize_device(psp_cu_handle* h, const double* d_velocity, int pan
     return Guard([&] { h->solver->Initialize(d_velocity, true, panel_scheme, precision); });
 }
 
+int psp_cu_initialize_batch(psp_cu_handle* const* h, const double* const* velocity, int count, int panel_scheme,
+                            int precision, int* failed) {
+    if (failed) *failed = -1;
+    if (count < 0 || (count > 0 && (!h || !velocity))) {
+        psp_b200::SetLastError("invalid batch");
+        return PSP_CU_LOGIC_ERROR;
+    }
+    for (int i = 0; i < count; ++i) {
+        if (int e = psp_cu_initialize(h[i], velocity[i], panel_scheme, precision)) {
+            if (failed) *failed = i;
+            return e;
+        }
+    }
+    return PSP_CU_OK;
+}
+
+int psp_cu_solve_batch(psp_cu_handle* const* h, double* const* B, const int* k, int count, int m, double rel_tol,
+                       psp_cu_stats* stats, int* failed) {
+    if (failed) *failed = -1;
+    if (count < 0 || (count > 0 && (!h || !B || !k))) {
+        psp_b200::SetLastError("invalid batch");
+        return PSP_CU_LOGIC_ERROR;
+    }
+    for (int i = 0; i < count; ++i) {
+        if (int e = psp_cu_solve(h[i], B[i], k[i], m, rel_tol, stats ? stats + i : nullptr)) {
+            if (failed) *failed = i;
+            return e;
+        }
+    }
+    return PSP_CU_OK;
+}
+
 int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_cu_stats* stats) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {

@@ -191,6 +191,41 @@ def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, pp
                          omega=omega, sources=centres, layer_tops=tops.tolist()))
 
 
+def batch_problems(count=48, seed=1003, sides=tuple(range(32, 97, 4)), pml=5, ppw_range=(8.0, 12.0),
+                   k_range=(1, 8), n_anom=3):
+    """Batching case: ``count`` independent problems, every side drawn from
+    ``sides`` (points including a ``pml``-point PML per face), a smooth
+    velocity in [0.6, 1.8] (background 1 plus seeded Gaussian anomalies),
+    omega giving U[8, 12] points per wavelength at the slowest velocity on
+    the coarsest axis, and k ~ U{1..8} Gaussian sources.  Returns
+    batch.Problem objects (natural order: velocity nx*ny*nz, rhs
+    nx*ny*nz x k)."""
+    from .batch import Problem
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        n = [int(rng.choice(sides)) for _ in range(3)]
+        interior = tuple(m - 2 * pml for m in n)
+        Zc, Yc, Xc = _grid(interior, pml)
+        vel = np.ones_like(Xc)
+        for _ in range(n_anom):
+            c = rng.uniform(0.15, 0.85, size=3)
+            amp = rng.uniform(-0.4, 0.6)
+            wid = rng.uniform(0.08, 0.2)
+            vel += amp * np.exp(-((Xc - c[0]) ** 2 + (Yc - c[1]) ** 2 + (Zc - c[2]) ** 2) / (2 * wid ** 2))
+        vel = np.clip(vel, 0.6, 1.8)
+        h = 1.0 / (min(interior) + 1)
+        ppw = rng.uniform(*ppw_range)
+        omega = 2 * math.pi * float(vel.min()) / (ppw * h)
+        k = int(rng.integers(k_range[0], k_range[1] + 1))
+        rhs, _ = gaussian_sources(interior, pml, k, rng)
+        disc = make_disc(interior, pml, omega)
+        out.append(Problem(disc, np.ascontiguousarray(vel).reshape(-1),
+                           np.ascontiguousarray(rhs).reshape(-1, k), "batch_%02d" % i,
+                           dict(sides=n, ppw=ppw, k=k)))
+    return out
+
+
 CONFIGS = {
     "plain_bump_50": plain_bump,
     "smooth_anomalies_116": smooth_anomalies,
