@@ -98,7 +98,8 @@ def test_two_gloo_ranks_share_and_gather_a_batch(tmp_path, monkeypatch):
     for r in range(2):
         got = np.load(tmp_path / ("rank%d.npz" % r))
         for i in range(len(probs)):
-            assert np.array_equal(got["arr_%d" % i], ref[i][0])
+            # same solves; BLAS threading may differ between the ranks and this process
+            assert np.linalg.norm(got["arr_%d" % i] - ref[i][0]) <= 1e-12 * np.linalg.norm(ref[i][0])
 
 
 @pytest.mark.gpu
