@@ -177,7 +177,20 @@ private:
     };
     std::vector<SweepGraph> graphs_;
     void SweepEager(z64* B, int ldk, int k);
-    void FactorGroup(int p0, int p1, FactorFront<R>* hostFronts, std::vector<FactorFront<R>>& all);
+    // The factorization of one group of panels as recorded launches: its
+    // transient buffers, uploaded task lists and steps.  When every panel
+    // fits in one group the program is kept, and a later Initialize of the
+    // same handle (same structure, new velocity) only replays it.
+    struct FactorProgram {
+        DeviceBuffer arena;
+        TaskArena tasks;
+        std::vector<Step> steps;
+        size_t frontsOff = 0;
+    };
+    std::vector<std::unique_ptr<FactorProgram>> program_;
+    void FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& all, bool keep);
+    void RunProgram(FactorProgram& pg);
+    void CheckPivots();
 
     Helmholtz& h_;
     const Analysis& an_;
@@ -210,6 +223,12 @@ private:
 
 template <typename R>
 void FactorStore<R>::Factor() {
+    if (!program_.empty()) {  // same structure as the last factorization: replay it
+        CUDA_CHECK(cudaMemsetAsync(status_.p, 0, sizeof(int), h_.stream_));
+        for (auto& pg : program_) RunProgram(*pg);
+        CheckPivots();
+        return;
+    }
     const PanelGeometry& g = an_.geom;
     const XYTree& tree = an_.tree;
     nn_ = (int)tree.nodes.size();
@@ -281,15 +300,21 @@ void FactorStore<R>::Factor() {
     const int64_t budget = (int64_t)(freeB * 0.8);
     int groupSize = np;
     while (groupSize > 1 && transient(0, groupSize) > budget) groupSize = (groupSize + 1) / 2;
-    for (int p0 = 0; p0 < np; p0 += groupSize) FactorGroup(p0, std::min(np, p0 + groupSize), nullptr, all);
-    int st = 0;
-    CUDA_CHECK(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, h_.stream_));
-    CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
-    if (st) throw PspError(kRuntimeError, "zero or non-finite pivot in a panel factorization");
+    for (int p0 = 0; p0 < np; p0 += groupSize)
+        FactorGroup(p0, std::min(np, p0 + groupSize), all, groupSize == np);
+    CheckPivots();
 }
 
 template <typename R>
-void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<FactorFront<R>>& all) {
+void FactorStore<R>::CheckPivots() {
+    int st = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, h_.stream_));
+    CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
+    if (st & 1) throw PspError(kRuntimeError, "zero or non-finite pivot in a panel factorization");
+}
+
+template <typename R>
+void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& all, bool keep) {
     const PanelGeometry& g = an_.geom;
     const XYTree& tree = an_.tree;
     const int nd = (int)depthNodes_.size();
@@ -314,7 +339,9 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
         lm = std::max(lm, Lsz[d]);
         tm = std::max(tm, Tsz[d]);
     }
-    DeviceBuffer arena;
+    std::unique_ptr<FactorProgram> pgHolder(new FactorProgram);
+    FactorProgram& pg = *pgHolder;
+    DeviceBuffer& arena = pg.arena;
     arena.Allocate((ua + ub + lm + tm) * sizeof(cpx<R>));
     cpx<R>* UA = arena.as<cpx<R>>();
     cpx<R>* UB = UA + ua;
@@ -330,9 +357,9 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
                 f.T = Tb + Tpos[i];
             }
 
-    TaskArena arenaTasks;
-    const size_t frontsOff = arenaTasks.Push(all);
-    std::vector<Step> steps;
+    TaskArena& arenaTasks = pg.tasks;
+    pg.frontsOff = arenaTasks.Push(all);
+    std::vector<Step>& steps = pg.steps;
     std::vector<GemmOp<R>> ops;
     std::vector<GemmTile> tiles;
     auto pushGemm = [&]() {
@@ -477,8 +504,17 @@ void FactorStore<R>::FactorGroup(int p0, int p1, FactorFront<R>*, std::vector<Fa
         pushGemm();
     }
     arenaTasks.Upload(st);
-    const FactorFront<R>* dFronts = arenaTasks.At<FactorFront<R>>(frontsOff);
-    for (const Step& s : steps) {
+    RunProgram(pg);
+    if (keep) program_.push_back(std::move(pgHolder));
+}
+
+template <typename R>
+void FactorStore<R>::RunProgram(FactorProgram& pg) {
+    cudaStream_t st = h_.stream_;
+    const DeviceBuffer& arena = pg.arena;
+    const TaskArena& arenaTasks = pg.tasks;
+    const FactorFront<R>* dFronts = arenaTasks.template At<FactorFront<R>>(pg.frontsOff);
+    for (const Step& s : pg.steps) {
         switch (s.kind) {
             case Step::kMemset:
                 if (s.bytes) CUDA_CHECK(cudaMemsetAsync((char*)arena.p + s.a, 0, s.bytes, st));
@@ -887,19 +923,24 @@ void Helmholtz::Initialize(const double* velocity, bool devicePtr, int panelSche
     if (panelScheme < 0 || panelScheme > 1) throw PspError(kLogicError, "Invalid panelScheme value");
     if (precision < 0 || precision > 1) throw PspError(kLogicError, "Invalid precision mode");
     if (!velocity) throw PspError(kLogicError, "Velocity grid is incorrect");
-    Finalize();
+    // A handle's discretization never changes, so a second Initialize at the
+    // same precision keeps the factor store (storage, recorded factorization,
+    // solve plans) and only refactors with the new velocity.
+    const bool reuse = precision == precision_ && (precision == 0 ? (bool)f64_ : (bool)f32_);
+    if (!reuse) Finalize();
+    initialized_ = false;
     const int64_t N = NumUnknowns();
-    dVel_.Allocate(N * sizeof(double));
+    if (!dVel_.p) dVel_.Allocate(N * sizeof(double));
     CUDA_CHECK(cudaMemcpyAsync(dVel_.p, velocity, N * sizeof(double),
                                devicePtr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
     ap_.vel = dVel_.as<double>();
     precision_ = precision;
     ProfilerBinding bind(&prof_);
     if (precision == 0) {
-        f64_.reset(new FactorStore<double>(*this));
+        if (!f64_) f64_.reset(new FactorStore<double>(*this));
         f64_->Factor();
     } else {
-        f32_.reset(new FactorStore<float>(*this));
+        if (!f32_) f32_.reset(new FactorStore<float>(*this));
         f32_->Factor();
     }
     CUDA_CHECK(cudaStreamSynchronize(stream_));

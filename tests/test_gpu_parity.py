@@ -153,3 +153,24 @@ def test_unit_cube_bump_property(product_lib):
     rr = max(np.linalg.norm(R[..., r]) / np.linalg.norm(w.rhs[..., r]) for r in range(w.k))
     assert rr < 1e-4
     assert abs(rr - st["final_max_rel_resid"]) < 1e-8
+
+
+@pytest.mark.gpu
+def test_reinitialize_matches_a_fresh_handle(product_lib):
+    """A second Initialize of a handle replays the recorded factorization
+    with the new velocity (and keeps solve plans); results must equal a fresh
+    handle's, also after switching precision in between."""
+    import psp_b200 as P
+    w = W.small_case()
+    v2 = np.asarray(w.velocity) * (1.0 + 0.05 * np.cos(np.arange(np.asarray(w.velocity).size)).reshape(
+        np.asarray(w.velocity).shape))
+    fresh = P.DistHelmholtz(w.disc)
+    fresh.Initialize(v2, precision=P.MIXED)
+    Xf = w.rhs.copy()
+    fresh.Solve(Xf, 20, 1e-8)
+    H = P.DistHelmholtz(w.disc)
+    for prec, vel in ((P.MIXED, w.velocity), (P.MIXED, v2), (P.FP64, w.velocity), (P.MIXED, v2)):
+        H.Initialize(vel, precision=prec)
+        X = w.rhs.copy()
+        H.Solve(X, 20, 1e-8)
+    assert np.array_equal(X, Xf)
