@@ -67,6 +67,30 @@ void AppendGemmTiles(const GemmOp<R>& op, int opIndex, GemmShape shape, std::vec
 template <typename R>
 void LaunchGemm(const GemmOp<R>* ops, const GemmTile* tiles, int numTiles, GemmShape shape, cudaStream_t st);
 
+// Tensor-core (tcgen05, split TF32) form of the complex-single batched GEMM
+// (factor_tc.cu) for ops with real alpha and beta: same op semantics, 128 x
+// 64 output tiles, each a self-contained record (operand pointers at the
+// tile's origin and the start of its K range), so the kernel reads one
+// record per tile and no op table.  A pipeline wait that times out sets the
+// value 2 in *status and leaves its tile unwritten.
+constexpr int kGemmTcRows = 128, kGemmTcCols = 64;
+struct GemmTcTile {
+    const c32* A;  // op(A)(row0, kb)
+    const c32* B;  // op(B)(kb, col0)
+    const c32* d;  // d + kb, or null
+    c32* C;        // C(row0, col0)
+    int lda, ldb, ldc;
+    int m, n, nk;  // rows and columns of the tile inside the op, K extent
+    int diag;      // lowerC: only tile-relative r - c >= diag is written
+    int flags;     // bit 0 transA, bit 1 transB
+    float alpha, beta;
+};
+// Whether `op` can take tensor-core tiles (real alpha and beta).
+bool GemmTcEligible(const GemmOp<float>& op);
+void PrepareFactorTcKernels();
+void AppendGemmTilesTc(const GemmOp<float>& op, std::vector<GemmTcTile>& tiles);
+void LaunchGemmTc(const GemmTcTile* tiles, int numTiles, int* status, cudaStream_t st);
+
 // ------------------------------------------------------------------ factorization
 
 constexpr int kNB = 32;  // column block of the frontal LDL^T

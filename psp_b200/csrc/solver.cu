@@ -141,6 +141,10 @@ public:
         const char* env = std::getenv("PSP_B200_SWEEP_CUDA_CORES");
         tc_ = std::is_same<R, float>::value && !(env && env[0] == '1');
         if (tc_) PrepareSweepTcKernels();
+        // Likewise the factorization GEMMs of complex-single fronts.
+        const char* fenv = std::getenv("PSP_B200_FACTOR_CUDA_CORES");
+        factorTc_ = std::is_same<R, float>::value && !(fenv && fenv[0] == '1');
+        if (factorTc_) PrepareFactorTcKernels();
     }
     ~FactorStore() {
         for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
@@ -165,8 +169,8 @@ public:
 private:
     struct Step {
         enum Kind { kMemset, kAssemble, kExtend, kDiag, kTrsm, kGemm } kind;
-        size_t a = 0, b = 0;
-        int n = 0, J = 0;
+        size_t a = 0, b = 0, c = 0;
+        int n = 0, nTc = 0, J = 0;  // n CUDA-core tiles at b, nTc tensor-core tiles at c
         size_t bytes = 0;
         double flops = 0, abytes = 0;
     };
@@ -218,6 +222,9 @@ private:
     std::vector<std::unique_ptr<SolvePlan>> plans_;
     SolvePlan& Plan(int k);
     bool tc_ = false;  // tensor-core sweep kernels (complex single only)
+    bool factorTc_ = false;  // tensor-core factorization GEMMs (complex single only)
+    // Ops of at least this many rows and K columns take tensor-core tiles.
+    bool UseGemmTc(const GemmOp<R>& op) const { return factorTc_ && op.M >= 64 && op.K >= 16; }
     int TileRows() const { return tc_ ? kTcRows : kSweepRows; }
 };
 
@@ -311,6 +318,7 @@ void FactorStore<R>::CheckPivots() {
     CUDA_CHECK(cudaMemcpyAsync(&st, status_.p, sizeof(int), cudaMemcpyDeviceToHost, h_.stream_));
     CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
     if (st & 1) throw PspError(kRuntimeError, "zero or non-finite pivot in a panel factorization");
+    if (st & 2) throw PspError(kRuntimeError, "a tensor-core pipeline wait timed out in the factorization");
 }
 
 template <typename R>
@@ -362,20 +370,34 @@ void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& al
     std::vector<Step>& steps = pg.steps;
     std::vector<GemmOp<R>> ops;
     std::vector<GemmTile> tiles;
+    std::vector<GemmTcTile> tilesTc;
     auto pushGemm = [&]() {
-        if (tiles.empty()) { ops.clear(); return; }
+        if (tiles.empty() && tilesTc.empty()) { ops.clear(); return; }
         Step s;
         s.kind = Step::kGemm;
         for (const GemmOp<R>& op : ops) OpCost(op, s.flops, s.abytes);
         s.a = arenaTasks.Push(ops);
-        s.b = arenaTasks.Push(tiles);
+        if (!tiles.empty()) s.b = arenaTasks.Push(tiles);
+        if (!tilesTc.empty()) s.c = arenaTasks.Push(tilesTc);
         s.n = (int)tiles.size();
+        s.nTc = (int)tilesTc.size();
         steps.push_back(s);
         ops.clear();
         tiles.clear();
+        tilesTc.clear();
+    };
+    // Tiles of `op` (index i) for the tensor-core or the CUDA-core kernel.
+    auto route = [&](const GemmOp<R>& op, int i, std::vector<GemmTile>& cc, std::vector<GemmTcTile>& tc) {
+        if constexpr (std::is_same<R, float>::value) {
+            if (UseGemmTc(op) && GemmTcEligible(op)) {
+                AppendGemmTilesTc(op, tc);
+                return;
+            }
+        }
+        AppendGemmTiles(op, i, kGemmSquare, cc);
     };
     auto addOp = [&](const GemmOp<R>& op) {
-        AppendGemmTiles(op, (int)ops.size(), kGemmSquare, tiles);
+        route(op, (int)ops.size(), tiles, tilesTc);
         ops.push_back(op);
     };
     const R one = 1, mone = -1, zero = 0;
@@ -462,6 +484,7 @@ void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& al
         for (int S = kNB; S < maxS; S *= 2) {
             std::vector<GemmOp<R>> ops2;
             std::vector<GemmTile> tiles2;
+            std::vector<GemmTcTile> tilesTc2;
             for (int fi : list) {
                 const FactorFront<R>& f = all[fi];
                 const int64_t ld = f.s + f.u;
@@ -479,13 +502,14 @@ void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& al
                     GemmOp<R> op2 = MakeOp<R>(f.G + a1 + a1 * lg, lg, 0, T, m, 0, f.G + a1 + a0 * lg, lg, m, n, m,
                                               mone, zero);
                     op2.triA = 1;
-                    AppendGemmTiles(op2, (int)ops2.size(), kGemmSquare, tiles2);
+                    route(op2, (int)ops2.size(), tiles2, tilesTc2);
                     ops2.push_back(op2);
                 }
             }
             pushGemm();
             ops = ops2;
             tiles = tiles2;
+            tilesTc = tilesTc2;
             pushGemm();
         }
         // G21 = -L21 inv(L11) and the Schur complement U -= L21 D L21^T
@@ -541,7 +565,11 @@ void FactorStore<R>::RunProgram(FactorProgram& pg) {
             }
             case Step::kGemm: {
                 ProfScope ps(st, kProfFactorGemm, s.flops, s.abytes);
-                LaunchGemm<R>(arenaTasks.At<GemmOp<R>>(s.a), arenaTasks.At<GemmTile>(s.b), s.n, kGemmSquare, st);
+                const GemmOp<R>* ops = arenaTasks.At<GemmOp<R>>(s.a);
+                if (s.n) LaunchGemm<R>(ops, arenaTasks.At<GemmTile>(s.b), s.n, kGemmSquare, st);
+                if constexpr (std::is_same<R, float>::value) {
+                    if (s.nTc) LaunchGemmTc(arenaTasks.At<GemmTcTile>(s.c), s.nTc, status_.as<int>(), st);
+                }
                 break;
             }
         }

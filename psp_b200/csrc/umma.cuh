@@ -58,6 +58,22 @@ __device__ __forceinline__ uint32_t Sw128Offset(int row, int chunk) {
     return (uint32_t)(row >> 3) * 1024u + (uint32_t)(row & 7) * 128u + (uint32_t)((chunk ^ (row & 7)) & 7) * 16u;
 }
 
+// The same in the 64-byte-swizzle layout: rows of 64 bytes (16 tf32 K
+// values), 8-row atoms of 512 bytes (512-byte aligned), chunk c of row r at
+// chunk position c ^ ((r / 2) % 4); +32 bytes selects the second K step.
+__device__ __forceinline__ uint64_t SmemDescSw64(uint32_t smemAddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smemAddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;            // leading byte offset (unused by swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;   // stride byte offset: one 8-row atom
+    d |= (uint64_t)1 << 46;            // descriptor version for sm100
+    d |= (uint64_t)4 << 61;            // SWIZZLE_64B
+    return d;
+}
+__device__ __forceinline__ uint32_t Sw64Offset(int row, int chunk) {
+    return (uint32_t)(row >> 3) * 512u + (uint32_t)(row & 7) * 64u + (uint32_t)((chunk ^ (row >> 1)) & 3) * 16u;
+}
+
 // Instruction descriptor: D f32, A and B tf32, both K-major, M x N.
 __host__ __device__ constexpr uint32_t InstrDescTf32(int M, int N) {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
