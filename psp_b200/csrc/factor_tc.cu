@@ -7,10 +7,9 @@
 // As in sweep_tc.cu, the complex product is one real product (A's rows as
 // interleaved (re, im) pairs, every B entry a 2x2 real block) and both
 // operands are split into tf32 head and tail; per 8-value K step
-//   MMA 1: A_hi [B_hi | B_lo]   (N = 256, accumulator columns 0-255)
-//   MMA 2: A_lo  B_hi           (N = 128, onto columns 0-127)
-// and the epilogue adds the two 128-column halves: hi*hi + hi*lo + lo*hi,
-// about FP32 accuracy.
+//   A_hi B_hi + A_hi B_lo + A_lo B_hi   (three N = 128 MMAs, one accumulator)
+// about FP32 accuracy.  A's split stage lives in tensor memory (the MMA
+// reads A from TMEM), so only B's planes take shared memory.
 //
 // Persistent and warp-specialized: CTA b takes tiles b, b + grid, ... (each
 // a 128 x 64 complex block described by one GemmTcTile record) and streams
@@ -18,10 +17,11 @@
 //   converters (8 warps)  asynchronous copies of operand stages into a
 //                         kRaw-slot ring kAhead stages ahead (zero-filled
 //                         outside the operands, any transposition), then the
-//                         split into one of two 64-byte-swizzled plane sets;
-//                         d scales B's rows here;
-//   MMA (one thread)      the split MMAs of a stage into one of two TMEM
-//                         accumulators; stage flags from the converters mark
+//                         split: A into TMEM (one lane per row), B into
+//                         one of two 64-byte-swizzled plane sets (d scales
+//                         B's rows here);
+//   MMA (one thread)      the split MMAs of a stage into one of two
+//                         128-column TMEM accumulators; stage flags mark
 //                         a tile's first and last stage;
 //   epilogue (4 warps)    one accumulator row per thread: alpha acc + beta C,
 //                         C staged in shared memory by copies issued while
@@ -45,9 +45,14 @@ constexpr int kFThreads = kMma0 + 32;
 constexpr int kRaw = 6, kAhead = kRaw - 1;  // raw slots; stages in flight ahead of the conversion
 constexpr int kPlaneSets = 2, kAccs = 2;
 
-constexpr uint32_t kAPl = kBM * 64;      // 8 KB: 128 rows of 16 tf32
-constexpr uint32_t kBPl = 2 * kBN * 64;  // 8 KB: B' has 2 kBN rows
-constexpr uint32_t kPlSet = 2 * kAPl + 2 * kBPl;  // A hi, A lo, B hi, B lo
+constexpr uint32_t kBPl = 2 * kBN * 64;  // 8 KB: B' has 2 kBN rows of 16 tf32
+constexpr uint32_t kPlSet = 2 * kBPl;     // B hi, B lo
+// TMEM columns: two accumulators of 2 kBN columns, then per plane set the
+// split A stage (head, then tail: 2 kSK columns each, lane = row)
+constexpr uint32_t kAccCols = 2 * kBN;
+constexpr uint32_t kACol0 = kAccs * kAccCols;
+constexpr uint32_t kACols = 2 * kSK;
+__host__ __device__ constexpr uint32_t ACol(int p) { return kACol0 + (uint32_t)p * 2 * kACols; }
 
 constexpr int kApad = kBM + 1, kBpad = kBN + 1;  // raw A [kc][row], raw B [kc][col]
 constexpr uint32_t kRawA = kSK * kApad * 8, kRawB = kSK * kBpad * 8;
@@ -55,13 +60,13 @@ constexpr uint32_t kRawSlot = kRawA + kRawB + kSK * 8;  // + d
 constexpr uint32_t kRawOff = kPlaneSets * kPlSet;
 constexpr uint32_t kStageOff = kRawOff + kRaw * kRawSlot;  // C staging [col][row]
 constexpr size_t kFactorTcSmem = kStageOff + (size_t)kBN * kBM * 8 + 1024;
-constexpr uint32_t kTmemCols = kAccs * 256;
-constexpr uint32_t kIdesc256 = umma::InstrDescTf32(kBM, 256);
-constexpr uint32_t kIdesc128 = umma::InstrDescTf32(kBM, 128);
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kIdesc = umma::InstrDescTf32(kBM, 2 * kBN);
 constexpr int kFirst = 1, kLast = 2;  // stage flags
 
 static_assert(kRawSlot % 16 == 0 && kStageOff % 16 == 0, "copy targets stay 16-byte aligned");
-static_assert(kPlSet % 1024 == 0 && kAPl % 512 == 0, "swizzle atoms stay aligned");
+static_assert(kPlSet % 1024 == 0 && kBPl % 512 == 0, "swizzle atoms stay aligned");
+static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
 static_assert(kFactorTcSmem <= 232448, "shared memory per CTA");
 static_assert(kConvThreads == 2 * kBM && kConvThreads == 4 * kBN, "converter thread mapping");
 
@@ -148,25 +153,29 @@ __device__ __forceinline__ void IssueStage(const GemmTcTile& T, int st, unsigned
 // complex K).  B: thread = (column c, chunk q): rows 2c, 2c+1 of B' hold the
 // 2x2 real blocks of complex K 2q, 2q+1; the first of the two stores goes to
 // row 2c or 2c+1 by bit 2 of c, so each store wave covers all banks.
-__device__ __forceinline__ void ConvertStage(const unsigned char* raw, unsigned char* P, int ct) {
+__device__ __forceinline__ void ConvertStage(const unsigned char* raw, unsigned char* P, uint32_t tmemA, int ct) {
     const c32* ra = reinterpret_cast<const c32*>(raw);
     const c32* rb = reinterpret_cast<const c32*>(raw + kRawA);
     const c32* rd = reinterpret_cast<const c32*>(raw + kRawA + kRawB);
     {
+        // row = this warp's TMEM lane quarter + lane; half h of the stage's K
         const int row = ct & (kBM - 1), h = ct / kBM;
+        float hi[8], lo[8];
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int chunk = 2 * h + j;
-            float2 h0, l0, h1, l1;
-            Split2(ra[(2 * chunk) * kApad + row], h0, l0);
-            Split2(ra[(2 * chunk + 1) * kApad + row], h1, l1);
-            const uint32_t off = umma::Sw64Offset(row, chunk);
-            *reinterpret_cast<float4*>(P + off) = make_float4(h0.x, h0.y, h1.x, h1.y);
-            *reinterpret_cast<float4*>(P + kAPl + off) = make_float4(l0.x, l0.y, l1.x, l1.y);
+        for (int j = 0; j < 4; ++j) {
+            float2 hv, lv;
+            Split2(ra[(4 * h + j) * kApad + row], hv, lv);
+            hi[2 * j] = hv.x;
+            hi[2 * j + 1] = hv.y;
+            lo[2 * j] = lv.x;
+            lo[2 * j + 1] = lv.y;
         }
+        const uint32_t at = tmemA + ((uint32_t)(row & ~31) << 16) + 8 * h;
+        umma::TmemStore8(at, hi);
+        umma::TmemStore8(at + kACols, lo);
     }
     {
-        unsigned char* bHi = P + 2 * kAPl;
+        unsigned char* bHi = P;
         unsigned char* bLo = bHi + kBPl;
         const int c = ct >> 2, q = ct & 3;
         const c32 b0 = rb[(2 * q) * kBpad + c] * rd[2 * q];
@@ -236,8 +245,10 @@ __device__ void ConverterRole(const GemmTcTile* tiles, int n, unsigned char* sme
         const int slot = g % kRaw;
         if (ct == 0) S.planeFlags[p] = S.rawFlags[slot];
         issueNext();
-        ConvertStage(raw + slot * kRawSlot, smem + p * kPlSet, ct);
+        ConvertStage(raw + slot * kRawSlot, smem + p * kPlSet, S.tmem + ACol(p), ct);
+        umma::TmemStoreWait();
         umma::FenceProxyAsync();
+        umma::FenceBeforeSync();
         umma::MbarArrive(&S.planeFull[p]);
     }
     umma::CpAsyncWaitAll();
@@ -256,14 +267,14 @@ __device__ void MmaRole(int n, unsigned char* smem, Sync& S, int* status) {
         const bool first = flags & kFirst;
         if (first && i >= kAccs && !Wait(&S.accEmpty[a], ((i / kAccs) - 1) & 1, S, status)) return;
         umma::FenceAfterSync();
-        const uint32_t acc = S.tmem + a * 256;
-        const uint32_t aHi = umma::SmemAddr(smem + p * kPlSet), aLo = aHi + kAPl, bHi = aHi + 2 * kAPl;
+        const uint32_t acc = S.tmem + a * kAccCols, aHi = S.tmem + ACol(p), aLo = aHi + kACols;
+        const uint32_t bHi = umma::SmemAddr(smem + p * kPlSet), bLo = bHi + kBPl;
 #pragma unroll
         for (int s = 0; s < 2 * kSK / 8; ++s) {
-            const uint32_t o = s * 32;
-            const uint64_t bd = umma::SmemDescSw64(bHi + o);
-            umma::MmaTf32(acc, umma::SmemDescSw64(aHi + o), bd, kIdesc256, (first && s == 0) ? 0u : 1u);
-            umma::MmaTf32(acc, umma::SmemDescSw64(aLo + o), bd, kIdesc128, 1u);
+            const uint64_t bh = umma::SmemDescSw64(bHi + 32 * s), bl = umma::SmemDescSw64(bLo + 32 * s);
+            umma::MmaTf32TmemA(acc, aHi + 8 * s, bh, kIdesc, (first && s == 0) ? 0u : 1u);
+            umma::MmaTf32TmemA(acc, aHi + 8 * s, bl, kIdesc, 1u);
+            umma::MmaTf32TmemA(acc, aLo + 8 * s, bh, kIdesc, 1u);
         }
         umma::CommitTo(&S.planeEmpty[p]);
         if (flags & kLast) {
@@ -287,8 +298,7 @@ __device__ __forceinline__ void IssueC(const GemmTcTile& T, c32* stage) {
 
 // alpha acc + beta C for this thread's row of 16 columns from column j0.
 template <bool kFull>
-__device__ __forceinline__ void StoreCols(const GemmTcTile& T, const float (&v0)[32], const float (&v1)[32],
-                                          const c32* stage, int j0) {
+__device__ __forceinline__ void StoreCols(const GemmTcTile& T, const float (&v)[32], const c32* stage, int j0) {
     const int r = threadIdx.x;
     c32* dst = T.C + r + (int64_t)j0 * T.ldc;
     const float al = T.alpha, be = T.beta;
@@ -296,7 +306,7 @@ __device__ __forceinline__ void StoreCols(const GemmTcTile& T, const float (&v0)
     for (int q = 0; q < 16; ++q, dst += T.ldc) {
         const int c = j0 + q;
         if (!kFull && (r >= T.m || c >= T.n || r - c < T.diag)) continue;
-        c32 out = mk(al * (v0[2 * q] + v1[2 * q]), al * (v0[2 * q + 1] + v1[2 * q + 1]));
+        c32 out = mk(al * v[2 * q], al * v[2 * q + 1]);
         if (be != 0.f) {
             const c32 cv = stage[c * kBM + r];
             out.re = fmaf(be, cv.re, out.re);
@@ -326,16 +336,15 @@ __device__ void EpilogueRole(const GemmTcTile* tiles, int n, c32* stage, Sync& S
         if (umma::NamedBarrierOr(2, kEpiThreads, !ok)) break;  // the staged C is visible
         umma::FenceAfterSync();
         const bool full = cur.m == kBM && cur.n == kBN && cur.diag <= 1 - kBN;
-        const uint32_t acc = S.tmem + lane + a * 256;
+        const uint32_t acc = S.tmem + lane + a * kAccCols;
 #pragma unroll 1
         for (int j = 0; j < kBN / 16; ++j) {
-            float v0[32], v1[32];
-            umma::TmemLoad32(acc + 32 * j, v0);
-            umma::TmemLoad32(acc + 128 + 32 * j, v1);
+            float v[32];
+            umma::TmemLoad32(acc + 32 * j, v);
             if (full)
-                StoreCols<true>(cur, v0, v1, stage, 16 * j);
+                StoreCols<true>(cur, v, stage, 16 * j);
             else
-                StoreCols<false>(cur, v0, v1, stage, 16 * j);
+                StoreCols<false>(cur, v, stage, 16 * j);
         }
         umma::FenceBeforeSync();
         umma::MbarArrive(&S.accEmpty[a]);

@@ -89,6 +89,18 @@ __device__ __forceinline__ void MmaTf32(uint32_t tmemD, uint64_t adesc, uint64_t
         : "r"(tmemD), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
+// The same with A read from tensor memory: M rows in TMEM lanes 0..M-1, one
+// tf32 K value per 32-bit column starting at column address tmemA.
+__device__ __forceinline__ void MmaTf32TmemA(uint32_t tmemD, uint32_t tmemA, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmemD), "r"(tmemA), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
 // Arrive on `mbar` once every tcgen05 operation issued so far by this thread
 // has completed.
 __device__ __forceinline__ void CommitTo(uint64_t* mbar) {
@@ -253,6 +265,17 @@ __device__ __forceinline__ void TmemStore32(uint32_t taddr, const float (&v)[32]
         : "memory");
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
+
+// Writes 8 consecutive 32-bit columns of this thread's TMEM lane without
+// waiting; TmemStoreWait() waits for all of this thread's TMEM stores.
+__device__ __forceinline__ void TmemStore8(uint32_t taddr, const float (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};\n" ::"r"(taddr),
+                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+                 : "memory");
+}
+__device__ __forceinline__ void TmemStoreWait() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // 16 consecutive f32 columns of this thread's TMEM lane.
 __device__ __forceinline__ void TmemLoad16(uint32_t taddr, float (&v)[16]) {
