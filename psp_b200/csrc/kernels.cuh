@@ -160,6 +160,7 @@ struct SweepFront {
     const int* rel;       // u rows of the structure in the parent front
     int s, u, ndOff, childSlot;
     int ldg;              // leading dimension of G (even)
+    const void* tmap;     // complex single: TMA maps of G (forward, backward; 128 bytes each)
 };
 
 // One CTA of a sweep launch: kSweepRows output rows from row0, kSweepCols
@@ -223,6 +224,10 @@ void LaunchSweepBackward(const SweepFront<R>* fr, const SweepTile* tiles, int n,
 // Tensor-core (tcgen05, split TF32) forms for complex-single factors
 // (sweep_tc.cu); tiles of kTcRows rows, any K-chunk length.
 void PrepareSweepTcKernels();
+// Bytes of the two TMA maps of one front, and their encoding (host) into
+// out (64-byte aligned host memory) for the front's G, s, u and ldg.
+constexpr size_t kSweepTcMapBytes = 256;
+void EncodeSweepTcMaps(const SweepFront<float>& f, void* out);
 void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, const SweepWork& w,
                           cudaStream_t st);
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k,

@@ -218,6 +218,10 @@ private:
         TaskArena arena;
         ClassPlan cplan[3];
         std::vector<size_t> panelFronts;
+        // complex single: the tensor-core sweep's TMA maps, two per front
+        struct alignas(64) MapPair { unsigned char b[kSweepTcMapBytes]; };
+        std::vector<MapPair> mapsHost;
+        DeviceBuffer maps;
     };
     std::vector<std::unique_ptr<SolvePlan>> plans_;
     SolvePlan& Plan(int k);
@@ -612,6 +616,10 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     P.Xnd.Allocate((size_t)maxSub * k * sizeof(cpx<R>));
     P.arena.host.clear();
     P.panelFronts.assign(np, 0);
+    if (tc_) {
+        P.mapsHost.assign((size_t)np * nn_, {});
+        P.maps.Allocate(P.mapsHost.size() * sizeof(typename SolvePlan::MapPair));
+    }
     for (int p = 0; p < np; ++p) {
         const int c = g.Class(p);
         const ClassStructure& cs = an_.cls[c];
@@ -632,6 +640,14 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             f.ndOff = cs.off[t];
             f.childSlot = (node.parent >= 0 && tree.nodes[node.parent].child[1] == t) ? 1 : 0;
             f.ldg = GLeadingDim(f.s, f.u);
+            f.tmap = nullptr;
+            if constexpr (std::is_same<R, float>::value) {
+                if (tc_ && f.s > 0) {
+                    const size_t i = (size_t)p * nn_ + t;
+                    EncodeSweepTcMaps(f, P.mapsHost[i].b);
+                    f.tmap = P.maps.template as<unsigned char>() + i * sizeof(typename SolvePlan::MapPair);
+                }
+            }
         }
         P.panelFronts[p] = P.arena.Push(fr);
     }
@@ -727,6 +743,8 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     P.counters.Allocate((size_t)maxCounters * sizeof(int));
     CUDA_CHECK(cudaMemsetAsync(P.counters.p, 0, P.counters.bytes, h_.stream_));
     P.arena.Upload(h_.stream_);
+    if (tc_)
+        CUDA_CHECK(cudaMemcpyAsync(P.maps.p, P.mapsHost.data(), P.maps.bytes, cudaMemcpyHostToDevice, h_.stream_));
     return P;
 }
 

@@ -17,15 +17,16 @@
 // one K-chunk, consumed in stages of 16 complex K-columns.  The kernels are
 // persistent (one CTA per SM walks the tiles blockIdx.x, blockIdx.x + grid,
 // ...) and warp-specialized, with mbarriers between the roles:
-//   producer (1 warp)   forward: bulk copies of G's 1 KB column segments
-//                       into a ring of kRaw raw stages (completion by
+//   producer (1 thread) one tiled TMA copy per stage of G's 128 x 16 box
+//                       (forward) or G^T's (backward), from two tensor maps
+//                       per front, into a ring of raw stages (completion by
 //                       transaction bytes)
-//   converters (8 warps) split raw stage g into tf32 head/tail planes
-//                       (128-byte swizzled K-major layout, kPlaneSets
-//                       buffers); each also copies its own right-hand-side
-//                       entries kAhead stages ahead, and in the backward
-//                       (128-byte rows of G^T, too short for bulk copies)
-//                       its own 16-byte chunks of A
+//   converters (8 warps) split raw stage g into tf32 head/tail: forward A
+//                       into TMEM (the MMA reads A from tensor memory),
+//                       backward A and both B's into 128-byte swizzled
+//                       K-major planes (kPlaneSets buffers); each also
+//                       copies its own right-hand-side entries kAhead
+//                       stages ahead
 //   MMA (1 thread)      tcgen05.mma per stage into one of kAccs TMEM
 //                       accumulators (round robin by tile)
 //   epilogue (4 warps)  TMEM -> registers, split-K reduction, and the result
@@ -36,6 +37,9 @@
 // Every wait on an mbarrier is bounded; a timeout sets bit 2 of the status
 // word and a shared abort flag that ends every role's loop; the CTA then
 // frees tensor memory and returns, leaving unfinished tiles unwritten.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "kernels.cuh"
 #include "umma.cuh"
 
@@ -60,7 +64,13 @@ constexpr uint32_t kPlaneSet = 2 * kAPlane + 2 * kBPlane;  // A hi, A lo, B hi, 
 constexpr int kPlaneSets = kGroups;                    // one per converter group
 constexpr uint32_t kAccCols = 4 * kSweepCols;          // f32 columns per accumulator (two halves)
 constexpr int kAccs = 4;                               // accumulators (tiles in flight per CTA)
-constexpr uint32_t kTmemCols = kAccs * kAccCols;
+// The forward kernel keeps each plane set's split A stage in TMEM after the
+// accumulators (head then tail, 2 kStageK columns each, lane = row): the MMA
+// reads A from tensor memory and only B's planes go through shared memory.
+constexpr uint32_t kAStageCols = 2 * kStageK;
+__host__ __device__ constexpr uint32_t ACol(int ps) { return kAccs * kAccCols + (uint32_t)ps * 2 * kAStageCols; }
+constexpr uint32_t kTmemCols = 512;
+static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
 constexpr uint32_t kIdescN64 = umma::InstrDescTf32(kTcRows, 4 * kSweepCols);
 constexpr uint32_t kIdescN32 = umma::InstrDescTf32(kTcRows, 2 * kSweepCols);
 
@@ -71,26 +81,41 @@ constexpr int kOutRowsPerPass = kEpiThreads / kSweepCols;  // 8
 constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 
 // Raw data of the stages in flight.
-//   forward:  A (G's column segments, [kc][row]) arrives by bulk copies
-//             into a ring of kRaw slots shared by both groups;
-//   each group: a ring of kOwn slots of its own copies (forward: B
-//             [plane][kc][n]; backward: A [row][kc] then B [kc][n]), every
-//             entry read back by the thread that copied it.
-constexpr int kRaw = 4;
+//   A arrives by one tiled TMA copy per stage into a ring of RawSlots(fwd)
+//   slots shared by both groups: forward G's 128-row x 16-column box
+//   ([kc][row]), backward G^T's 128 x 16 box ([row][kc]).  The forward keeps
+//   A in TMEM, so its last four slots reuse the A planes of the plane sets.
+//   Each group: a ring of kOwn slots of its own copies of B (forward
+//   [plane][kc][n], backward [kc][n]), every entry read back by the thread
+//   that copied it.
+constexpr int kRawMax = 8;
+__host__ __device__ constexpr int RawSlots(bool fwd) { return fwd ? 8 : 6; }
+__host__ __device__ constexpr int RawInRegion(bool fwd) { return fwd ? 4 : 6; }
 constexpr int kAheadOwn = 2;                           // own stages in flight per group
 constexpr int kOwn = kAheadOwn + 1;
 constexpr uint32_t kRawA = kStageK * kTcRows * 8;      // 16 KB
 __host__ __device__ constexpr uint32_t OwnSlot(bool fwd) {
-    return fwd ? 3 * kStageK * kSweepCols * 8 : kRawA + kStageK * kSweepCols * 8;
+    return fwd ? 3 * kStageK * kSweepCols * 8 : kStageK * kSweepCols * 8;
 }
-__host__ __device__ constexpr uint32_t OwnBase(bool fwd) { return fwd ? kRaw * kRawA : 0; }
+__host__ __device__ constexpr uint32_t OwnBase(bool fwd) { return RawInRegion(fwd) * kRawA; }
 constexpr uint32_t kRegionOff = kPlaneSets * kPlaneSet;
+static_assert(RawSlots(true) - RawInRegion(true) == 2 * kPlaneSets && kRawA == kAPlane,
+              "the forward's extra raw slots are the plane sets' A planes");
 constexpr uint32_t kRegion =
     (OwnBase(true) + kGroups * kOwn * OwnSlot(true)) > (OwnBase(false) + kGroups * kOwn * OwnSlot(false))
         ? (OwnBase(true) + kGroups * kOwn * OwnSlot(true))
         : (OwnBase(false) + kGroups * kOwn * OwnSlot(false));
 constexpr uint32_t kStagingOff = kRegionOff + kRegion;
 constexpr size_t kTcSmem = kStagingOff + kStaging + 1024;
+static_assert(kTcSmem <= 232448, "shared memory per CTA");
+
+// Raw A slot `slot` (shared-memory base `smem`, 1 KB aligned).
+template <bool kFwd>
+__device__ __forceinline__ unsigned char* RawSlotPtr(unsigned char* smem, int slot) {
+    if (slot < RawInRegion(kFwd)) return smem + kRegionOff + slot * kRawA;
+    const int e = slot - RawInRegion(kFwd);
+    return smem + (e / 2) * kPlaneSet + (e % 2) * kAPlane;
+}
 
 // Stage description handed from the loaders to the MMA thread.
 struct StageHdr {
@@ -100,10 +125,10 @@ struct StageHdr {
 struct Sync {
     uint64_t planeFull[kPlaneSets], planeEmpty[kPlaneSets];
     uint64_t accFull[kAccs], accEmpty[kAccs];
-    uint64_t rawFull[kRaw], rawEmpty[kRaw];
+    uint64_t rawFull[kRawMax], rawEmpty[kRawMax];
     StageHdr hdr[kPlaneSets];
     int ownInfo[kGroups][kOwn];  // stage place, packed (see InfoSt); written and read by a group's first thread
-    int rawK[kRaw][2];           // stage's first K index and the tile's K end
+    int rawK[kRawMax][2];        // stage's first K index and the tile's K end
     uint32_t tmem;
     int abort;
     int isLast;
@@ -163,6 +188,7 @@ constexpr int kFrontLag = 2;
 struct LoadMeta {
     const c32* G;
     const c32* B;  // forward: Rb; backward: Z
+    const void* tmap;  // forward map of the front (the backward map follows it)
     int ld, rows, row0, col0, kb, ke, nst;
 };
 
@@ -178,12 +204,14 @@ struct LoadCursor {
     LoadMeta m;
     int nFront, nRow0, nCol0, nK0, nK1;  // next tile
     const c32 *nG, *nB;                  // its front
+    const void* nMap;
     int ns, nu, haveNt, haveNf;
 
     __device__ __forceinline__ void SetMeta(int row0, int col0, int k0, int k1, const c32* G, const c32* B, int s,
-                                            int u) {
+                                            int u, const void* tmap) {
         m.G = G;
         m.B = B;
+        m.tmap = tmap;
         m.ld = GLeadingDim(s, u);
         m.rows = kFwd ? s + u : s;
         m.row0 = row0;
@@ -200,7 +228,7 @@ struct LoadCursor {
         if (total == 0) return;
         const SweepTile t = tiles[ti];
         const SweepFront<float>& f = fr[t.front];
-        SetMeta(t.row0, t.col0, t.k0, t.k1, f.G, kFwd ? f.Rb : f.Z, f.s, f.u);
+        SetMeta(t.row0, t.col0, t.k0, t.k1, f.G, kFwd ? f.Rb : f.Z, f.s, f.u, f.tmap);
         PrefetchTile();
     }
     __device__ __forceinline__ void PrefetchTile() {
@@ -216,6 +244,7 @@ struct LoadCursor {
             const SweepFront<float>& f = fr[nFront];
             nG = f.G;
             nB = kFwd ? f.Rb : f.Z;
+            nMap = f.tmap;
             ns = f.s;
             nu = f.u;
             haveNf = 1;
@@ -237,61 +266,37 @@ struct LoadCursor {
         st = 0;
         if (ti >= n) { total = gl; return; }
         PrefetchFront();
-        SetMeta(nRow0, nCol0, nK0, nK1, nG, nB, ns, nu);
+        SetMeta(nRow0, nCol0, nK0, nK1, nG, nB, ns, nu, nMap);
         PrefetchTile();
     }
 };
 
 // ------------------------------------------------------------------ producer
 
-// One warp copies each stage's A operand with bulk copies of contiguous
-// segments of G: forward, up to 16 K-columns of up to 128 rows (rounded up
-// to an even count, which G's even leading dimension keeps inside the
-// column); backward, up to 128 rows of G^T of 16 K-values.  Lane 0 arms the
-// slot's barrier with the byte count before any lane copies.
+// Lane 0 of one warp copies each stage's A operand with one tiled TMA copy of
+// the front's map: forward the 128-row x 16-column box of G at (row0,
+// kBase), backward the 16 x 128 box of G at (kBase, row0), i.e. 128 rows of
+// G^T.  Rows or columns outside G arrive as zeros; K columns past the tile's
+// range are masked by the converters.
 template <bool kFwd>
 __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
-                             int k, unsigned char* raw, Sync& S, int* status) {
-    const int lane = threadIdx.x & 31;
+                             int k, unsigned char* smem, Sync& S, int* status) {
+    if ((threadIdx.x & 31) != 0) return;
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
     for (int g = 0; cur.Valid(g); ++g) {
-        const int slot = g % kRaw;
-        if (g >= kRaw && !Wait(&S.rawEmpty[slot], ((g / kRaw) - 1) & 1, S, status)) return;
+        const int slot = g % RawSlots(kFwd);
+        if (g >= RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / RawSlots(kFwd)) - 1) & 1, S, status)) return;
         const LoadMeta& m = cur.m;
         const int kBase = cur.KBase();
-        uint32_t bytes;
-        if (kFwd) {
-            const int rows = min(kTcRows, m.rows - m.row0);
-            const int ncols = min(kStageK, m.ke - kBase);
-            bytes = (ncols > 0 && rows > 0) ? (uint32_t)ncols * (uint32_t)((rows + 1) & ~1) * 8u : 0u;
-        } else {
-            const int rows = min(kTcRows, m.rows - m.row0);
-            const int ncols = min(kStageK, m.ke - kBase);
-            bytes = (ncols > 0 && rows > 0) ? (uint32_t)rows * (uint32_t)((ncols + 1) & ~1) * 8u : 0u;
-        }
-        if (lane == 0) {
-            S.rawK[slot][0] = kBase;
-            S.rawK[slot][1] = m.ke;
-            umma::MbarArriveExpectTx(&S.rawFull[slot], bytes);
-        }
-        __syncwarp();
-        unsigned char* dst = raw + slot * kRawA;
-        if (bytes) {
-            if (kFwd) {
-                const int rows2 = (min(kTcRows, m.rows - m.row0) + 1) & ~1;
-                const int ncols = min(kStageK, m.ke - kBase);
-                if (lane < ncols)
-                    umma::BulkCopy(dst + lane * kTcRows * 8, m.G + m.row0 + (int64_t)(kBase + lane) * m.ld,
-                                   (uint32_t)rows2 * 8u, &S.rawFull[slot]);
-            } else {
-                const int rows = min(kTcRows, m.rows - m.row0);
-                const int ncols2 = (min(kStageK, m.ke - kBase) + 1) & ~1;
-                for (int r = lane; r < rows; r += 32)
-                    umma::BulkCopy(dst + r * kStageK * 8, m.G + kBase + (int64_t)(m.row0 + r) * m.ld,
-                                   (uint32_t)ncols2 * 8u, &S.rawFull[slot]);
-            }
-        }
+        S.rawK[slot][0] = kBase;
+        S.rawK[slot][1] = m.ke;
+        umma::MbarArriveExpectTx(&S.rawFull[slot], kRawA);
+        const unsigned char* map = reinterpret_cast<const unsigned char*>(m.tmap) + (kFwd ? 0 : 128);
+        if (kFwd)
+            umma::TmaLoad2D(RawSlotPtr<kFwd>(smem, slot), map, m.row0, kBase, &S.rawFull[slot]);
+        else
+            umma::TmaLoad2D(RawSlotPtr<kFwd>(smem, slot), map, kBase, m.row0, &S.rawFull[slot]);
         cur.Advance();
     }
 }
@@ -319,7 +324,7 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
     const int ct = (threadIdx.x - kLoad0) % kGroupThreads;
     if (ct == 0) S.ownInfo[gr][slot] = cur.Info();
     unsigned char* base = own + slot * OwnSlot(kFwd);
-    c32* rb = reinterpret_cast<c32*>(base + (kFwd ? 0 : kRawA));
+    c32* rb = reinterpret_cast<c32*>(base);
     const int ncol = min(kSweepCols, cur.k - m.col0);
     const int kBase = cur.KBase();
 #pragma unroll
@@ -337,17 +342,6 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
             umma::CpAsync8(rb + e, ok ? m.B + (int64_t)kk * cur.k + m.col0 + nn : m.B, ok ? 8u : 0u);
         }
     }
-    if (!kFwd) {
-        c32* ra = reinterpret_cast<c32*>(base);
-#pragma unroll
-        for (int i = 0; i < kStageK * kTcRows / 2 / kGroupThreads; ++i) {
-            const int c = ct + i * kGroupThreads;
-            const int mm = c / (kStageK / 2), q = c % (kStageK / 2);
-            const int rr = m.row0 + mm, kk0 = kBase + 2 * q;
-            const int nv = (rr < m.rows) ? max(0, min(2, m.ke - kk0)) : 0;
-            umma::CpAsync16(ra + mm * kStageK + 2 * q, nv ? m.G + kk0 + (int64_t)rr * m.ld : m.G, 8u * nv);
-        }
-    }
     umma::CpAsyncCommit();
 #pragma unroll
     for (int i = 0; i < kGroups; ++i) cur.Advance();
@@ -357,39 +351,44 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
 // K-columns at or beyond kValid are taken as zero.
 template <bool kFwd>
 __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawA, const unsigned char* own,
-                                             int kValid, int ct) {
+                                             int kValid, int ct, uint32_t tmemA) {
     unsigned char* aHi = P;
     unsigned char* aLo = P + kAPlane;
     const c32 zero = mk<float>(0, 0);
     if (kFwd) {
+        // thread ct = row = TMEM lane ct of this warp's lane quarter
         const c32* ra = reinterpret_cast<const c32*>(rawA);
         const int row = ct;
+        float hi[2 * kStageK], lo[2 * kStageK];
 #pragma unroll
-        for (int q = 0; q < kStageK / 2; ++q) {  // chunk: complex K 2q, 2q+1
-            float2 h0, l0, h1, l1;
-            Split2(2 * q < kValid ? ra[(2 * q) * kTcRows + row] : zero, h0, l0);
-            Split2(2 * q + 1 < kValid ? ra[(2 * q + 1) * kTcRows + row] : zero, h1, l1);
-            const uint32_t off = umma::Sw128Offset(row, q);
-            *reinterpret_cast<float4*>(aHi + off) = make_float4(h0.x, h0.y, h1.x, h1.y);
-            *reinterpret_cast<float4*>(aLo + off) = make_float4(l0.x, l0.y, l1.x, l1.y);
+        for (int kc = 0; kc < kStageK; ++kc) {
+            float2 h, l;
+            Split2(kc < kValid ? ra[kc * kTcRows + row] : zero, h, l);
+            hi[2 * kc] = h.x;
+            hi[2 * kc + 1] = h.y;
+            lo[2 * kc] = l.x;
+            lo[2 * kc + 1] = l.y;
         }
+        const uint32_t at = tmemA + ((uint32_t)(row & ~31) << 16);
+        umma::TmemStore32NoWait(at, hi);
+        umma::TmemStore32NoWait(at + kAStageCols, lo);
     } else {
-        // this thread's own chunks (already zero-filled outside the tile)
-        const c32* ra = reinterpret_cast<const c32*>(own);
+        // G^T rows from the raw ring ([row][kc]); K past the tile's range is zero
+        const c32* ra = reinterpret_cast<const c32*>(rawA);
 #pragma unroll
         for (int i = 0; i < kStageK * kTcRows / 2 / kGroupThreads; ++i) {
             const int c = ct + i * kGroupThreads;
             const int m = c / (kStageK / 2), q = c % (kStageK / 2);
             float2 h0, l0, h1, l1;
-            Split2(ra[m * kStageK + 2 * q], h0, l0);
-            Split2(ra[m * kStageK + 2 * q + 1], h1, l1);
+            Split2(2 * q < kValid ? ra[m * kStageK + 2 * q] : zero, h0, l0);
+            Split2(2 * q + 1 < kValid ? ra[m * kStageK + 2 * q + 1] : zero, h1, l1);
             const uint32_t off = umma::Sw128Offset(m, q);
             *reinterpret_cast<float4*>(aHi + off) = make_float4(h0.x, h0.y, h1.x, h1.y);
             *reinterpret_cast<float4*>(aLo + off) = make_float4(l0.x, l0.y, l1.x, l1.y);
         }
     }
     // B: entry (kc, n) becomes rows 2n, 2n+1 of B' at K positions 2kc, 2kc+1
-    const c32* rb = reinterpret_cast<const c32*>(own + (kFwd ? 0 : kRawA));
+    const c32* rb = reinterpret_cast<const c32*>(own);
     unsigned char* bHi = P + 2 * kAPlane;
     unsigned char* bLo = bHi + kBPlane;
 #pragma unroll
@@ -413,15 +412,19 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
 template <bool kFwd>
 __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char* own, const LoadCursor<kFwd>& cur,
                                               int g, int gr, int ct, Sync& S, int* status) {
-    const int ps = gr, slot = g % kRaw, oslot = (g / kGroups) % kOwn;
+    const int ps = gr, slot = g % RawSlots(kFwd), oslot = (g / kGroups) % kOwn;
     const bool valid = cur.Valid(g);
-    if (kFwd && valid && !Wait(&S.rawFull[slot], (g / kRaw) & 1, S, status)) return false;
+    if (valid && !Wait(&S.rawFull[slot], (g / RawSlots(kFwd)) & 1, S, status)) return false;
     if (g >= kGroups && !Wait(&S.planeEmpty[ps], ((g / kGroups) - 1) & 1, S, status)) return false;
     umma::CpAsyncWait<kAheadOwn>();  // this thread's own copies of stage g have landed
     if (valid) {
-        const int kValid = kFwd ? S.rawK[slot][1] - S.rawK[slot][0] : kStageK;
-        ConvertStage<kFwd>(smem + ps * kPlaneSet, smem + kRegionOff + slot * kRawA, own + oslot * OwnSlot(kFwd),
-                           kValid, ct);
+        const int kValid = S.rawK[slot][1] - S.rawK[slot][0];
+        ConvertStage<kFwd>(smem + ps * kPlaneSet, RawSlotPtr<kFwd>(smem, slot), own + oslot * OwnSlot(kFwd),
+                           kValid, ct, S.tmem + ACol(ps));
+    }
+    if (kFwd) {
+        umma::TmemStoreWait();
+        umma::FenceBeforeSync();
     }
     umma::FenceProxyAsync();
     if (ct == 0) {
@@ -429,7 +432,7 @@ __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char
         S.hdr[ps] = valid ? StageHdr{1, InfoSt(info), InfoNst(info), InfoJ(info)} : StageHdr{0, 0, 0, 0};
     }
     umma::MbarArrive(&S.planeFull[ps]);
-    if (kFwd && valid) umma::MbarArrive(&S.rawEmpty[slot]);
+    if (valid) umma::MbarArrive(&S.rawEmpty[slot]);
     return valid;
 }
 
@@ -455,14 +458,21 @@ __device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const Sw
 
 // `init`: the accumulator starts from its current contents (the forward
 // epilogue preloads it); otherwise the tile's first MMA overwrites it.
-__device__ __forceinline__ void IssueStage(const unsigned char* P, uint32_t tmem, bool init) {
+// Forward: A's split stage is read from TMEM at tmemA (head, then tail).
+template <bool kFwd>
+__device__ __forceinline__ void IssueStage(const unsigned char* P, uint32_t tmem, uint32_t tmemA, bool init) {
     const uint32_t aHi = umma::SmemAddr(P), aLo = aHi + kAPlane, bHi = aHi + 2 * kAPlane;
 #pragma unroll
     for (int s = 0; s < 2 * kStageK / 8; ++s) {
         const uint32_t o = s * 32;
         const uint64_t bd = umma::SmemDescSw128(bHi + o);
-        umma::MmaTf32(tmem, umma::SmemDescSw128(aHi + o), bd, kIdescN64, (init || s > 0) ? 1u : 0u);
-        umma::MmaTf32(tmem, umma::SmemDescSw128(aLo + o), bd, kIdescN32, 1u);
+        if (kFwd) {
+            umma::MmaTf32TmemA(tmem, tmemA + 8 * s, bd, kIdescN64, (init || s > 0) ? 1u : 0u);
+            umma::MmaTf32TmemA(tmem, tmemA + kAStageCols + 8 * s, bd, kIdescN32, 1u);
+        } else {
+            umma::MmaTf32(tmem, umma::SmemDescSw128(aHi + o), bd, kIdescN64, (init || s > 0) ? 1u : 0u);
+            umma::MmaTf32(tmem, umma::SmemDescSw128(aLo + o), bd, kIdescN32, 1u);
+        }
     }
 }
 
@@ -476,7 +486,7 @@ __device__ void MmaRole(const unsigned char* planes, Sync& S, int* status) {
         const int b = h.j % kAccs;
         if (h.st == 0 && !Wait(&S.accEmpty[b], (h.j / kAccs) & 1, S, status)) return;
         umma::FenceAfterSync();
-        IssueStage(planes + ps * kPlaneSet, S.tmem + b * kAccCols, kFwd || h.st > 0);
+        IssueStage<kFwd>(planes + ps * kPlaneSet, S.tmem + b * kAccCols, S.tmem + ACol(ps), kFwd || h.st > 0);
         umma::CommitTo(&S.planeEmpty[ps]);
         if (h.st == h.nst - 1) umma::CommitTo(&S.accFull[b]);
     }
@@ -657,7 +667,7 @@ __device__ __forceinline__ void InitSync(Sync& S) {
             umma::MbarInit(&S.accFull[i], 1);
             umma::MbarInit(&S.accEmpty[i], kEpiThreads);
         }
-        for (int i = 0; i < kRaw; ++i) {
+        for (int i = 0; i < kRawMax; ++i) {
             umma::MbarInit(&S.rawFull[i], 1);
             umma::MbarInit(&S.rawEmpty[i], kGroupThreads);
         }
@@ -698,7 +708,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
     } else if (tid == kMma0) {
         MmaRole<true>(smem, S, work.status);
     } else if (tid >= kProd0) {
-        ProducerRole<true>(fr, tiles, n, k, smem + kRegionOff, S, work.status);
+        ProducerRole<true>(fr, tiles, n, k, smem, S, work.status);
     }
     Teardown(S);
 }
@@ -717,6 +727,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const 
         ConverterRole<false>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
         MmaRole<false>(smem, S, work.status);
+    } else if (tid >= kProd0) {
+        ProducerRole<false>(fr, tiles, n, k, smem, S, work.status);
     }
     Teardown(S);
 }
@@ -726,6 +738,34 @@ int g_numSMs = 0;
 int GridFor(int n) { return n < g_numSMs ? n : g_numSMs; }
 
 }  // namespace
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 g_encodeTiled = nullptr;
+}
+
+void EncodeSweepTcMaps(const SweepFront<float>& f, void* out) {
+    if (!g_encodeTiled) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        CUDA_CHECK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) throw PspError(kCudaError, "cuTensorMapEncodeTiled is unavailable");
+        g_encodeTiled = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    // G as a (s+u) x s array of 8-byte complex-single entries, column stride
+    // ldg (even, so every column starts on a 16-byte boundary)
+    const cuuint64_t dims[2] = {(cuuint64_t)(f.s + f.u), (cuuint64_t)f.s};
+    const cuuint64_t strides[1] = {(cuuint64_t)f.ldg * sizeof(c32)};
+    const cuuint32_t unit[2] = {1, 1};
+    const cuuint32_t boxes[2][2] = {{(cuuint32_t)kTcRows, (cuuint32_t)kStageK}, {(cuuint32_t)kStageK, (cuuint32_t)kTcRows}};
+    CUtensorMap* maps = static_cast<CUtensorMap*>(out);
+    for (int b = 0; b < 2; ++b) {
+        const CUresult r = g_encodeTiled(&maps[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<c32*>(f.G), dims,
+                                         strides, boxes[b], unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) throw PspError(kCudaError, "cuTensorMapEncodeTiled failed for a sweep front");
+    }
+}
 
 void PrepareSweepTcKernels() {
     int dev = 0;

@@ -215,6 +215,19 @@ __device__ __forceinline__ void BulkCopy(void* dst, const void* src, uint32_t by
         "l"(src), "r"(bytes), "r"(SmemAddr(mbar))
         : "memory");
 }
+// Tiled 2-D tensor copy (no multicast) of the box at coordinates (x, y) of
+// the tensor map at `tmap` (global memory, 64-byte aligned) into this CTA's
+// shared memory (128-byte aligned), completing as transaction bytes on
+// `mbar`; elements outside the tensor are zero-filled.  x * element size
+// must be a multiple of 16 bytes.
+__device__ __forceinline__ void TmaLoad2D(void* dst, const void* tmap, int x, int y, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(SmemAddr(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(SmemAddr(mbar))
+        : "memory");
+}
+
 // Arrive on `mbar` and add `bytes` to the transaction bytes its phase waits for.
 __device__ __forceinline__ void MbarArriveExpectTx(uint64_t* mbar, uint32_t bytes) {
     asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
@@ -244,6 +257,25 @@ __device__ __forceinline__ bool NamedBarrierOr(int id, int nthreads, bool pred) 
         : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
         : "memory");
     return r != 0;
+}
+
+// Writes 32 consecutive f32 columns of this thread's TMEM lane without
+// waiting (TmemStoreWait() waits for all of this thread's TMEM stores).
+__device__ __forceinline__ void TmemStore32NoWait(uint32_t taddr, const float (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};\n"
+        ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+        "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+        "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15])),
+        "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])), "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])),
+        "r"(__float_as_uint(v[20])), "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+        "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])), "r"(__float_as_uint(v[27])),
+        "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])), "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+        : "memory");
 }
 
 // Writes 32 consecutive f32 columns of this thread's TMEM lane and waits
