@@ -2,6 +2,7 @@
 // CUDA error plumbing that turns every failure into an exception carrying a
 // psp status code (the C ABI converts it back into a return code).
 #pragma once
+#include <utility>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -91,5 +92,30 @@ inline void CudaCheck(cudaError_t e, const char* what, const char* file, int lin
 #define CUDA_LAUNCH_CHECK() ::psp_b200::CudaCheck(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
 
 inline unsigned CeilDiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// Programmatic dependent launch.  A kernel launched with LaunchPdl may start
+// while the kernel before it in the stream is still running: it calls
+// PdlTrigger() so that the kernel after it may be scheduled likewise, and
+// PdlWait() (which returns once the preceding kernel has completed and its
+// memory is visible) before touching any data that kernel reads or writes.
+// A dependent grid starts only after every block of its predecessor has
+// triggered, so waiting blocks never hold back unscheduled ones.
+__device__ __forceinline__ void PdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void PdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+void LaunchPdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CudaCheck(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...), "kernel launch", __FILE__, __LINE__);
+}
 
 }  // namespace psp_b200

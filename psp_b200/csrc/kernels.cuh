@@ -207,16 +207,17 @@ int SweepMaxChunk();
 // Sets kernel attributes the sweep kernels need (call before any graph capture).
 template <typename R>
 void PrepareSweepKernels();
-// tasks: (front, first row), kSweepRows rows each
+// tasks: (front, first row), kSweepRows rows each.  `pdl`: launch as a
+// programmatic dependent of the preceding kernel (the tensor-core sweep).
 template <typename R>
 void LaunchSweepPregather(const SweepFront<R>* fr, const int2* tasks, int n, const z64* B, int k, const PanelIO& io,
-                          cudaStream_t st);
+                          cudaStream_t st, bool pdl = false);
 template <typename R>
 void LaunchSweepForward(const SweepFront<R>* fr, const SweepTile* tiles, int n, int maxChunk, int k,
                         const SweepWork& w, cudaStream_t st);
 template <typename R>
 void LaunchSweepBackwardGather(const SweepFront<R>* fr, const int2* tasks, int n, int k, const SweepWork& w,
-                               cudaStream_t st);
+                               cudaStream_t st, bool pdl = false);
 template <typename R>
 void LaunchSweepBackward(const SweepFront<R>* fr, const SweepTile* tiles, int n, int maxChunk, z64* B, int k,
                          const PanelIO& io, const SweepWork& w, cudaStream_t st);

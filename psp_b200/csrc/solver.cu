@@ -777,7 +777,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     const int nd = (int)depthNodes_.size();
     {
         ProfScope ps(st, kProfGatherScatter);
-        LaunchSweepPregather<R>(fr, P.arena.template At<int2>(cp.pre), cp.preN, B, k, io, st);
+        LaunchSweepPregather<R>(fr, P.arena.template At<int2>(cp.pre), cp.preN, B, k, io, st, tc_);
     }
     for (int d = nd - 1; d >= 0; --d) {
         ProfScope ps(st, kProfSolveGemm, cp.fFlops[d], cp.fBytes[d]);
@@ -793,7 +793,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     for (int d = 0; d < nd; ++d) {
         {
             ProfScope ps(st, kProfGatherScatter);
-            LaunchSweepBackwardGather<R>(fr, P.arena.template At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st);
+            LaunchSweepBackwardGather<R>(fr, P.arena.template At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st, tc_);
         }
         ProfScope ps(st, kProfSolveGemm, cp.bFlops[d], cp.bBytes[d]);
         const SweepTile* tl = P.arena.template At<SweepTile>(cp.bTiles[d]);

@@ -173,6 +173,8 @@ __global__ void __launch_bounds__(kGatherThreads) sweep_pregather_kernel(const S
                                                                          const int2* __restrict__ tasks,
                                                                          const z64* __restrict__ B, int k,
                                                                          PanelIO io) {
+    PdlTrigger();
+    PdlWait();
     const int2 task = tasks[blockIdx.x];
     const SweepFront<R> f = fr[task.x];
     const int rows = min(kSweepRows, f.s + f.u - task.y);
@@ -236,6 +238,8 @@ template <typename R>
 __global__ void __launch_bounds__(kGatherThreads) sweep_bgather_kernel(const SweepFront<R>* __restrict__ fr,
                                                                        const int2* __restrict__ tasks, int k,
                                                                        SweepWork work) {
+    PdlTrigger();
+    PdlWait();
     const int2 task = tasks[blockIdx.x];
     const SweepFront<R> f = fr[task.x];
     const cpx<R>* X = reinterpret_cast<const cpx<R>*>(work.xnd);
@@ -319,8 +323,12 @@ void PrepareSweepKernels() {
 
 template <typename R>
 void LaunchSweepPregather(const SweepFront<R>* fr, const int2* tasks, int n, const z64* B, int k, const PanelIO& io,
-                          cudaStream_t st) {
+                          cudaStream_t st, bool pdl) {
     if (n <= 0) return;
+    if (pdl) {
+        LaunchPdl(sweep_pregather_kernel<R>, dim3(n), dim3(kGatherThreads), 0, st, fr, tasks, B, k, io);
+        return;
+    }
     sweep_pregather_kernel<R><<<n, kGatherThreads, 0, st>>>(fr, tasks, B, k, io);
     CUDA_LAUNCH_CHECK();
 }
@@ -335,8 +343,12 @@ void LaunchSweepForward(const SweepFront<R>* fr, const SweepTile* tiles, int n, 
 
 template <typename R>
 void LaunchSweepBackwardGather(const SweepFront<R>* fr, const int2* tasks, int n, int k, const SweepWork& w,
-                               cudaStream_t st) {
+                               cudaStream_t st, bool pdl) {
     if (n <= 0) return;
+    if (pdl) {
+        LaunchPdl(sweep_bgather_kernel<R>, dim3(n), dim3(kGatherThreads), 0, st, fr, tasks, k, w);
+        return;
+    }
     sweep_bgather_kernel<R><<<n, kGatherThreads, 0, st>>>(fr, tasks, k, w);
     CUDA_LAUNCH_CHECK();
 }
@@ -353,11 +365,11 @@ void LaunchSweepBackward(const SweepFront<R>* fr, const SweepTile* tiles, int n,
     template int SweepMaxChunk<R>();                                                                              \
     template void PrepareSweepKernels<R>();                                                                       \
     template void LaunchSweepPregather<R>(const SweepFront<R>*, const int2*, int, const z64*, int, const PanelIO&, \
-                                          cudaStream_t);                                                          \
+                                          cudaStream_t, bool);                                                    \
     template void LaunchSweepForward<R>(const SweepFront<R>*, const SweepTile*, int, int, int, const SweepWork&,  \
                                         cudaStream_t);                                                            \
     template void LaunchSweepBackwardGather<R>(const SweepFront<R>*, const int2*, int, int, const SweepWork&,     \
-                                               cudaStream_t);                                                     \
+                                               cudaStream_t, bool);                                               \
     template void LaunchSweepBackward<R>(const SweepFront<R>*, const SweepTile*, int, int, z64*, int,           \
                                          const PanelIO&, const SweepWork&, cudaStream_t);
 

@@ -445,6 +445,7 @@ __device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const Sw
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
     for (int i = 0; i < gr; ++i) cur.Advance();
+    PdlWait();  // right-hand sides come from the preceding kernels
 #pragma unroll
     for (int a = 0; a < kAheadOwn; ++a) IssueOwn(cur, own, gr, S);
     for (int g = gr;; g += kGroups) {
@@ -608,6 +609,7 @@ __device__ void EpilogueRole(const SweepFront<float>* __restrict__ fr, const Swe
     const int warp = threadIdx.x / 32, row = threadIdx.x;
     c32* X = reinterpret_cast<c32*>(w.xnd);
     int ti;
+    PdlWait();  // carries, split-K scratch and outputs are shared with the preceding kernels
     // set up the first kAccs accumulators
     for (int q = 0; q < kAccs && TileOf(tiles, n, q, ti); ++q) {
         if (kFwd) {
@@ -699,6 +701,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
                                                                          int k, SweepWork work) {
     __shared__ Sync S;
     unsigned char* smem = SmemBase();
+    PdlTrigger();
     InitSync(S);
     const int tid = threadIdx.x;
     if (tid < kLoad0) {
@@ -719,6 +722,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const 
                                                                           SweepWork work) {
     __shared__ Sync S;
     unsigned char* smem = SmemBase();
+    PdlTrigger();
     InitSync(S);
     const int tid = threadIdx.x;
     if (tid < kLoad0) {
@@ -780,14 +784,14 @@ void PrepareSweepTcKernels() {
 void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, const SweepWork& w,
                           cudaStream_t st) {
     if (n <= 0) return;
-    sweep_tc_forward_kernel<<<GridFor(n), kTcThreads, kTcSmem, st>>>(fr, tiles, n, k, w);
+    LaunchPdl(sweep_tc_forward_kernel, dim3(GridFor(n)), dim3(kTcThreads), kTcSmem, st, fr, tiles, n, k, w);
     CUDA_LAUNCH_CHECK();
 }
 
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k,
                            const PanelIO& io, const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    sweep_tc_backward_kernel<<<GridFor(n), kTcThreads, kTcSmem, st>>>(fr, tiles, n, B, k, io, w);
+    LaunchPdl(sweep_tc_backward_kernel, dim3(GridFor(n)), dim3(kTcThreads), kTcSmem, st, fr, tiles, n, B, k, io, w);
     CUDA_LAUNCH_CHECK();
 }
 
