@@ -423,6 +423,10 @@ def main():
         vel_h = np.ascontiguousarray(w.velocity.reshape(-1))
         rhs_h = np.ascontiguousarray(w.rhs.reshape(-1))
         B_h = np.empty_like(rhs_h)
+        # one untimed call: the handle's pinned staging and device scratch
+        H.Initialize(vel_h, precision=P.MIXED)
+        B_h[:] = rhs_h
+        H.Solve(B_h, RESTART, REL_TOL)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier(ws)
         torch.cuda.synchronize()

@@ -57,18 +57,19 @@ void FillStats(const psp_b200::SolveStats& s, psp_cu_stats* out) {
     out->num_preconditions = s.numPreconditions;
 }
 
-// Runs fn on a device copy of the host grid B and copies the result back.
+// Runs fn on a device copy of the host grid B and copies the result back,
+// through the handle's pinned staging and device scratch.
 template <typename F>
-void OnDeviceCopy(Helmholtz* s, double* B, int k, F&& fn) {
+void OnDeviceCopy(psp_cu_handle* h, double* B, int k, F&& fn) {
     if (!B) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
     if (k < 1) throw PspError(PSP_CU_LOGIC_ERROR, "need at least one right-hand side");
+    Helmholtz* s = h->solver;
+    CUDA_CHECK(cudaSetDevice(s->device()));
     const size_t bytes = (size_t)s->NumUnknowns() * k * 2 * sizeof(double);
-    psp_b200::DeviceBuffer d;
-    d.Allocate(bytes);
-    CUDA_CHECK(cudaMemcpyAsync(d.p, B, bytes, cudaMemcpyHostToDevice, s->stream()));
-    fn(d.as<psp_b200::z64>());
-    CUDA_CHECK(cudaMemcpyAsync(B, d.p, bytes, cudaMemcpyDeviceToHost, s->stream()));
-    CUDA_CHECK(cudaStreamSynchronize(s->stream()));
+    void* d = h->io.Device(bytes);
+    h->io.ToDevice(d, B, bytes, s->stream());
+    fn(static_cast<psp_b200::z64*>(d));
+    h->io.ToHost(B, d, bytes, s->stream());
 }
 
 }  // namespace
@@ -105,7 +106,15 @@ void psp_cu_destroy(psp_cu_handle* h) {
 
 int psp_cu_initialize(psp_cu_handle* h, const double* velocity, int panel_scheme, int precision) {
     if (int e = CheckHandle(h)) return e;
-    return Guard([&] { h->solver->Initialize(velocity, false, panel_scheme, precision); });
+    return Guard([&] {
+        // argument errors are reported by Initialize itself, in its order
+        if (!velocity) return h->solver->Initialize(nullptr, false, panel_scheme, precision);
+        CUDA_CHECK(cudaSetDevice(h->solver->device()));
+        const size_t bytes = (size_t)h->solver->NumUnknowns() * sizeof(double);
+        void* d = h->io.Device(bytes);
+        h->io.ToDevice(d, velocity, bytes, h->solver->stream());
+        h->solver->Initialize(static_cast<const double*>(d), true, panel_scheme, precision);
+    });
 }
 
 int psp_cu_initialize_device(psp_cu_handle* h, const double* d_velocity, int panel_scheme, int precision) {
@@ -150,7 +159,7 @@ int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_
     return Guard([&] {
         if (!h->solver->Initialized()) throw PspError(PSP_CU_NOT_INITIALIZED, "DistHelmholtz is not initialized");
         psp_b200::SolveStats s;
-        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->SolveDevice(d, k, m, rel_tol, &s); });
+        OnDeviceCopy(h, B, k, [&](psp_b200::z64* d) { h->solver->SolveDevice(d, k, m, rel_tol, &s); });
         FillStats(s, stats);
     });
 }
@@ -173,7 +182,7 @@ int psp_cu_finalize(psp_cu_handle* h) {
 int psp_cu_multiply(psp_cu_handle* h, double* B, int k) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {
-        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->MultiplyDevice(d, k); });
+        OnDeviceCopy(h, B, k, [&](psp_b200::z64* d) { h->solver->MultiplyDevice(d, k); });
     });
 }
 
@@ -181,7 +190,7 @@ int psp_cu_precondition(psp_cu_handle* h, double* B, int k) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {
         if (!h->solver->Initialized()) throw PspError(PSP_CU_NOT_INITIALIZED, "DistHelmholtz is not initialized");
-        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->PreconditionDevice(d, k); });
+        OnDeviceCopy(h, B, k, [&](psp_b200::z64* d) { h->solver->PreconditionDevice(d, k); });
     });
 }
 
@@ -208,7 +217,7 @@ int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {
         if (!h->solver->Initialized()) throw PspError(PSP_CU_NOT_INITIALIZED, "DistHelmholtz is not initialized");
-        OnDeviceCopy(h->solver, B, k, [&](psp_b200::z64* d) { h->solver->SolvePanelDevice(d, k, panel); });
+        OnDeviceCopy(h, B, k, [&](psp_b200::z64* d) { h->solver->SolvePanelDevice(d, k, panel); });
     });
 }
 

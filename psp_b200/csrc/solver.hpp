@@ -91,6 +91,7 @@ public:
     const Analysis& analysis() const { return an_; }
     int64_t NumUnknowns() const { return (int64_t)an_.disc.nx * an_.disc.ny * an_.disc.nz; }
     cudaStream_t stream() const { return stream_; }
+    int device() const { return device_; }
     int precision() const { return precision_; }
     double setupSeconds() const { return setupSeconds_; }
     int64_t factorBytes() const;
