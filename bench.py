@@ -55,9 +55,43 @@ def parse():
     ap.add_argument("--no-grad", action="store_true", help="skip the gradients/s arm")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch-of-48-problems arm")
     ap.add_argument("--grad-config", default="layered_faults_96")
+    ap.add_argument("--grid-probe", action="store_true",
+                    help="time grid ingest: a ZYX-ordered velocity file loaded to the device and resampled 2x")
     ap.add_argument("--sweep-probe", action="store_true",
                     help="profiling driver: Initialize (mixed) + two sweeps on the device, then exit")
     return ap.parse_args()
+
+
+def grid_probe(args):
+    """Grid ingest on the device (SequentialLoad + InterpolateTo): the
+    workload's velocity written as a ZYX-ordered binary file, loaded back
+    in natural order, then resampled to twice the points per axis.  Times
+    from CUDA events around the (synchronous) C-ABI calls; bytes are the
+    file bytes (load: host read, copy and reorder) and the interpolation's
+    output bytes plus one read of its input."""
+    import torch
+    import psp_b200 as P
+    w = workload(args.config)
+    nx, ny, nz = w.disc.nx, w.disc.ny, w.disc.nz
+    path = os.path.join(tempfile.mkdtemp(), "velocity_zyx.bin")
+    # ZYX order: z fastest, then y, then x
+    np.ascontiguousarray(w.velocity.reshape(nz, ny, nx).transpose(2, 1, 0)).tofile(path)
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for rep in range(3):  # the last repetition is reported
+        e[0].record()
+        vel = P.load_grid(path, nx, ny, nz, 1, P.ZYX)
+        e[1].record()
+        e[2].record()
+        big = P.interpolate_grid(vel, (nx, ny, nz), (2 * nx, 2 * ny, 2 * nz))
+        e[3].record()
+        torch.cuda.synchronize()
+    os.remove(path)
+    n0, n1 = nx * ny * nz, 8 * nx * ny * nz
+    t_load, t_int = e[0].elapsed_time(e[1]) * 1e-3, e[2].elapsed_time(e[3]) * 1e-3
+    print(json.dumps({"probe": "grid_ingest", "grid": [nx, ny, nz], "load_s": t_load,
+                      "load_gbs": 8 * n0 / t_load / 1e9, "interpolate_to": [2 * nx, 2 * ny, 2 * nz],
+                      "interpolate_s": t_int, "interpolate_gbs": 8 * (n0 + n1) / t_int / 1e9,
+                      "checksum": float(big.sum())}), flush=True)
 
 
 def sweep_probe(args):
@@ -382,6 +416,8 @@ def main_reference(args):
 
 def main():
     args = parse()
+    if args.grid_probe:
+        return grid_probe(args)
     if args.sweep_probe:
         return sweep_probe(args)
     if args.impl == "reference":

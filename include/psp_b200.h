@@ -181,6 +181,40 @@ int psp_cu_sweep_cost(const psp_cu_handle* h, int k, double* flops, double* byte
 int psp_cu_analyze_class(const psp_cu_disc* disc, int planes_per_panel, int cutoff, int cls, int* num_nodes,
                          int* vsize, int* info, int* nd_to_nat);
 
+/* ---- grid ingest and output (psp::DistUniformGrid on one process) ------
+ * A grid is nx*ny*nz points with num_scalars values per point (is_complex:
+ * each value is two doubles, re and im), natural order unless stated.
+ * Storage orders are the reference's GridDataOrder: 0 XYZ, 1 XZY, 2 YXZ,
+ * 3 YZX, 4 ZXY, 5 ZYX (axes fastest to slowest); plane types are its
+ * PlaneType: 0 XY, 1 XZ, 2 YZ. */
+
+/* DistUniformGrid::SequentialLoad (dist_uniform_grid.hpp:349-482): reads the
+ * binary file (stored in `order`) and writes the grid in natural order to
+ * d_out (device memory of the current device), reordering on the device.
+ * LOGIC_ERROR when the file cannot be opened or is shorter than the grid. */
+int psp_cu_grid_load(const char* filename, int nx, int ny, int nz, int num_scalars, int is_complex, int order,
+                     double* d_out);
+
+/* DistUniformGrid::InterpolateTo (dist_uniform_grid.hpp:484-714): trilinear
+ * resampling of d_in (old sizes) to d_out (new sizes), both device memory of
+ * the current device; equal sizes copy.  Each value component is
+ * interpolated with the reference's weights and operation order. */
+int psp_cu_grid_interpolate(const double* d_in, int nx_old, int ny_old, int nz_old, int num_scalars, int is_complex,
+                            double* d_out, int nx, int ny, int nz);
+
+/* DistUniformGrid::WritePlane (dist_uniform_grid.hpp:716-1631): ASCII VTK
+ * ImageData of plane `which_plane` of host grid data, one file per scalar,
+ * basename_k.vti (complex: basename_k_real.vti and basename_k_imag.vti).
+ * LOGIC_ERROR "Invalid plane" when the plane index is out of range. */
+int psp_cu_grid_write_plane(const double* data, int nx, int ny, int nz, int num_scalars, int is_complex,
+                            int plane_type, int which_plane, const char* basename);
+
+/* DistUniformGrid::WriteVolume (dist_uniform_grid.hpp:1788-2200) for one
+ * process: per scalar a basename_k.pvti description (complex: _real and
+ * _imag) whose piece is basename_k/0.vti, from host grid data. */
+int psp_cu_grid_write_volume(const double* data, int nx, int ny, int nz, int num_scalars, int is_complex,
+                             const char* basename);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ PML, DIRICHLET = 0, 1
 CLIQUE_LDL_1D, CLIQUE_LDL_SELINV_1D = 0, 1
 FP64, MIXED = 0, 1
 XYZ, XZY, YXZ, YZX, ZXY, ZYX = range(6)
+XY, XZ, YZ = range(3)  # PlaneType (dist_uniform_grid.hpp:24-28)
 
 _STATUS = {0: "ok", 1: "logic error", 2: "runtime error", 3: "CUDA error", 4: "out of memory",
            5: "not initialized", 6: "no CUDA device"}
@@ -72,6 +73,7 @@ C_ABI_SYMBOLS = [
     "psp_cu_geometry", "psp_cu_setup_info", "psp_cu_analyze_class", "psp_cu_get_stream",
     "psp_cu_set_profiling", "psp_cu_profile_reset", "psp_cu_profile_get", "psp_cu_sweep_cost",
     "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device", "psp_cu_initialize_batch", "psp_cu_solve_batch",
+    "psp_cu_grid_load", "psp_cu_grid_interpolate", "psp_cu_grid_write_plane", "psp_cu_grid_write_volume",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -120,6 +122,11 @@ def lib():
                                               ctypes.c_int, ip]
         L.psp_cu_solve_batch.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(dp), ip, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_double, ctypes.POINTER(_Stats), ip]
+        ci = ctypes.c_int
+        L.psp_cu_grid_load.argtypes = [ctypes.c_char_p, ci, ci, ci, ci, ci, ci, vp]
+        L.psp_cu_grid_interpolate.argtypes = [vp, ci, ci, ci, ci, ci, vp, ci, ci, ci]
+        L.psp_cu_grid_write_plane.argtypes = [dp, ci, ci, ci, ci, ci, ci, ci, ctypes.c_char_p]
+        L.psp_cu_grid_write_volume.argtypes = [dp, ci, ci, ci, ci, ci, ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -222,6 +229,40 @@ class DistUniformGrid:
         v = np.transpose(a.reshape(*dims, numScalars), perm + (3,))
         return cls(nx, ny, nz, numScalars, dtype, v)
 
+    def _is_complex(self):
+        return np.iscomplexobj(self.data)
+
+    def SequentialLoad(self, filename, order=XYZ):
+        """Fill the grid from a binary file stored in GridDataOrder ``order``
+        (SequentialLoad, dist_uniform_grid.hpp:349-482); the file is
+        reordered on the GPU (device 0 unless torch's current device)."""
+        t = load_grid(filename, self.nx, self.ny, self.nz, self.numScalars, order, self._is_complex())
+        self.data = np.ascontiguousarray(t.cpu().numpy()).reshape(self.nz, self.ny, self.nx, self.numScalars)
+
+    def InterpolateTo(self, nx, ny, nz):
+        """Trilinear resampling to nx x ny x nz (InterpolateTo,
+        dist_uniform_grid.hpp:484-714), computed on the GPU."""
+        import torch
+        src = torch.from_numpy(self.data.reshape(-1)).cuda()
+        out = interpolate_grid(src, (self.nx, self.ny, self.nz), (nx, ny, nz), self.numScalars)
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.data = np.ascontiguousarray(out.cpu().numpy()).reshape(self.nz, self.ny, self.nx, self.numScalars)
+
+    def WritePlane(self, planeType, whichPlane, basename):
+        """ASCII VTK files of one plane, one per scalar (WritePlane,
+        dist_uniform_grid.hpp:716-1631)."""
+        a = np.ascontiguousarray(self.data)
+        _check(lib().psp_cu_grid_write_plane(_dptr(a.view(np.float64)), self.nx, self.ny, self.nz, self.numScalars,
+                                             int(self._is_complex()), int(planeType), int(whichPlane),
+                                             str(basename).encode()))
+
+    def WriteVolume(self, basename):
+        """ASCII VTK volume files, one .pvti + piece per scalar (WriteVolume,
+        dist_uniform_grid.hpp:1788-2200, one process)."""
+        a = np.ascontiguousarray(self.data)
+        _check(lib().psp_cu_grid_write_volume(_dptr(a.view(np.float64)), self.nx, self.ny, self.nz, self.numScalars,
+                                              int(self._is_complex()), str(basename).encode()))
+
 
 def analyze_class(disc, planes_per_panel=4, cutoff=12, cls=0):
     """Host-only symbolic analysis of one panel class: returns (info, ndToNat)
@@ -236,6 +277,42 @@ def analyze_class(disc, planes_per_panel=4, cutoff=12, cls=0):
     _check(lib().psp_cu_analyze_class(ctypes.byref(d), planes_per_panel, cutoff, cls, ctypes.byref(n),
                                       ctypes.byref(vs), _iptr(info), _iptr(nd)))
     return info.reshape(n.value, 4), nd
+
+
+def load_grid(filename, nx, ny, nz, numScalars=1, order=XYZ, is_complex=False, device=None):
+    """A binary grid file stored in GridDataOrder ``order`` as a CUDA tensor
+    in natural order, shape (nz, ny, nx, numScalars), float64 or complex128
+    (SequentialLoad, dist_uniform_grid.hpp:349-482; the reorder runs on the
+    GPU)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    dtype = torch.complex128 if is_complex else torch.float64
+    out = torch.empty((nz, ny, nx, numScalars), dtype=dtype, device=dev)
+    with torch.cuda.device(dev):
+        torch.cuda.synchronize()
+        _check(lib().psp_cu_grid_load(str(filename).encode(), nx, ny, nz, numScalars, int(is_complex), int(order),
+                                      ctypes.c_void_p(out.data_ptr())))
+    return out
+
+
+def interpolate_grid(grid, old_sizes, new_sizes, numScalars=1):
+    """Trilinear resampling of a natural-order CUDA grid (float64 or
+    complex128, nx*ny*nz*numScalars values) from old_sizes = (nx, ny, nz) to
+    new_sizes (InterpolateTo, dist_uniform_grid.hpp:484-714); returns a new
+    tensor of shape (nz, ny, nx, numScalars)."""
+    import torch
+    src = grid.contiguous()
+    nx0, ny0, nz0 = (int(v) for v in old_sizes)
+    nx, ny, nz = (int(v) for v in new_sizes)
+    if src.numel() != nx0 * ny0 * nz0 * numScalars:
+        raise LogicError("grid size does not match its dimensions")
+    is_complex = src.is_complex()
+    out = torch.empty((nz, ny, nx, numScalars), dtype=src.dtype, device=src.device)
+    with torch.cuda.device(src.device):
+        torch.cuda.synchronize()
+        _check(lib().psp_cu_grid_interpolate(ctypes.c_void_p(src.data_ptr()), nx0, ny0, nz0, numScalars,
+                                             int(is_complex), ctypes.c_void_p(out.data_ptr()), nx, ny, nz))
+    return out
 
 
 class DistHelmholtz:

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "../../include/psp_b200.h"
+#include "grid_io.hpp"
 #include "handle.hpp"
 #include "solver.hpp"
 
@@ -315,6 +316,38 @@ int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* 
     if (setup_seconds) *setup_seconds = h->solver->setupSeconds();
     if (factor_bytes) *factor_bytes = (long long)h->solver->factorBytes();
     return PSP_CU_OK;
+}
+
+int psp_cu_grid_load(const char* filename, int nx, int ny, int nz, int num_scalars, int is_complex, int order,
+                     double* d_out) {
+    return Guard([&] {
+        if (!filename) throw PspError(PSP_CU_LOGIC_ERROR, "null file name");
+        psp_b200::GridLoad(filename, nx, ny, nz, num_scalars * (is_complex ? 2 : 1), order, d_out);
+    });
+}
+
+int psp_cu_grid_interpolate(const double* d_in, int nx_old, int ny_old, int nz_old, int num_scalars, int is_complex,
+                            double* d_out, int nx, int ny, int nz) {
+    return Guard([&] {
+        psp_b200::GridInterpolate(d_in, nx_old, ny_old, nz_old, num_scalars * (is_complex ? 2 : 1), d_out, nx, ny,
+                                  nz);
+    });
+}
+
+int psp_cu_grid_write_plane(const double* data, int nx, int ny, int nz, int num_scalars, int is_complex,
+                            int plane_type, int which_plane, const char* basename) {
+    return Guard([&] {
+        if (!basename) throw PspError(PSP_CU_LOGIC_ERROR, "null base name");
+        psp_b200::GridWritePlane(data, nx, ny, nz, num_scalars, is_complex != 0, plane_type, which_plane, basename);
+    });
+}
+
+int psp_cu_grid_write_volume(const double* data, int nx, int ny, int nz, int num_scalars, int is_complex,
+                             const char* basename) {
+    return Guard([&] {
+        if (!basename) throw PspError(PSP_CU_LOGIC_ERROR, "null base name");
+        psp_b200::GridWriteVolume(data, nx, ny, nz, num_scalars, is_complex != 0, basename);
+    });
 }
 
 }  // extern "C"
