@@ -24,6 +24,7 @@ enum Boundary { PML = PSP_CU_PML, DIRICHLET = PSP_CU_DIRICHLET };
 enum PanelScheme { CLIQUE_LDL_1D = PSP_CU_LDL_1D, CLIQUE_LDL_SELINV_1D = PSP_CU_LDL_SELINV_1D };
 enum Precision { FP64 = PSP_CU_FP64, MIXED = PSP_CU_MIXED };
 enum GridDataOrder { XYZ, XZY, YXZ, YZX, ZXY, ZYX };
+enum PlaneType { XY, XZ, YZ };  // dist_uniform_grid.hpp:24-28
 
 namespace detail {
 inline void Check(int code) {
@@ -88,10 +89,38 @@ struct Discretization {
 template <typename F>
 class DistUniformGrid {
 public:
+    // The buffer is always held in natural (XYZ) order; `order` is the layout
+    // of the files SequentialLoad reads (dist_uniform_grid.hpp:349-482).
     DistUniformGrid(int nx, int ny, int nz, int /*device*/ = 0, int numScalars = 1, GridDataOrder order = XYZ)
         : nx_(nx), ny_(ny), nz_(nz), numScalars_(numScalars), order_(order),
-          data_((size_t)nx * ny * nz * numScalars) {
-        if (order != XYZ) throw std::logic_error("only the XYZ storage order is held in memory");
+          data_((size_t)nx * ny * nz * numScalars) {}
+
+    // SequentialLoad (dist_uniform_grid.hpp:349-482): the file, stored in the
+    // grid's order, reordered on the GPU into this buffer.
+    void SequentialLoad(const std::string& filename) {
+        detail::Check(psp_cu_grid_load(filename.c_str(), nx_, ny_, nz_, numScalars_, kComplex, order_,
+                                       reinterpret_cast<double*>(data_.data())));
+    }
+    // InterpolateTo (dist_uniform_grid.hpp:484-714), computed on the GPU.
+    void InterpolateTo(int nx, int ny, int nz) {
+        if (nx == nx_ && ny == ny_ && nz == nz_) return;
+        std::vector<F> out((size_t)nx * ny * nz * numScalars_);
+        detail::Check(psp_cu_grid_interpolate(reinterpret_cast<const double*>(data_.data()), nx_, ny_, nz_,
+                                              numScalars_, kComplex, reinterpret_cast<double*>(out.data()), nx,
+                                              ny, nz));
+        data_.swap(out);
+        nx_ = nx;
+        ny_ = ny;
+        nz_ = nz;
+    }
+    // WritePlane / WriteVolume (dist_uniform_grid.hpp:716-2200): ASCII VTK.
+    void WritePlane(PlaneType planeType, int whichPlane, const std::string& basename) const {
+        detail::Check(psp_cu_grid_write_plane(reinterpret_cast<const double*>(data_.data()), nx_, ny_, nz_,
+                                              numScalars_, kComplex, planeType, whichPlane, basename.c_str()));
+    }
+    void WriteVolume(const std::string& basename) const {
+        detail::Check(psp_cu_grid_write_volume(reinterpret_cast<const double*>(data_.data()), nx_, ny_, nz_,
+                                               numScalars_, kComplex, basename.c_str()));
     }
     int XSize() const { return nx_; }
     int YSize() const { return ny_; }
@@ -114,6 +143,7 @@ public:
     GridDataOrder Order() const { return order_; }
 
 private:
+    static constexpr int kComplex = sizeof(F) == 2 * sizeof(double) ? 1 : 0;
     int nx_, ny_, nz_, numScalars_;
     GridDataOrder order_;
     std::vector<F> data_;

@@ -190,15 +190,17 @@ int psp_cu_analyze_class(const psp_cu_disc* disc, int planes_per_panel, int cuto
 
 /* DistUniformGrid::SequentialLoad (dist_uniform_grid.hpp:349-482): reads the
  * binary file (stored in `order`) and writes the grid in natural order to
- * d_out (device memory of the current device), reordering on the device.
+ * d_out, reordering on the current device; d_out may be device memory or
+ * host memory (then staged through a temporary device buffer).
  * LOGIC_ERROR when the file cannot be opened or is shorter than the grid. */
 int psp_cu_grid_load(const char* filename, int nx, int ny, int nz, int num_scalars, int is_complex, int order,
                      double* d_out);
 
 /* DistUniformGrid::InterpolateTo (dist_uniform_grid.hpp:484-714): trilinear
- * resampling of d_in (old sizes) to d_out (new sizes), both device memory of
- * the current device; equal sizes copy.  Each value component is
- * interpolated with the reference's weights and operation order. */
+ * resampling of d_in (old sizes) to d_out (new sizes) on the current device;
+ * equal sizes copy.  Either may be host memory (then staged through
+ * temporary device buffers).  Each value component is interpolated with the
+ * reference's weights and operation order. */
 int psp_cu_grid_interpolate(const double* d_in, int nx_old, int ny_old, int nz_old, int num_scalars, int is_complex,
                             double* d_out, int nx, int ny, int nz);
 

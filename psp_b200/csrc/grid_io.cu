@@ -109,6 +109,22 @@ int IoGrid(int64_t total) {
     return (int)std::min<int64_t>(b, 148 * 16);
 }
 
+bool OnDevice(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();  // not a pointer CUDA knows: host memory
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// A device buffer of n doubles freed on scope exit.
+struct DeviceDoubles {
+    double* p = nullptr;
+    explicit DeviceDoubles(size_t n) { CUDA_CHECK(cudaMalloc(&p, n * sizeof(double))); }
+    ~DeviceDoubles() { cudaFree(p); }
+};
+
 void CheckSizes(int nx, int ny, int nz, int doubles) {
     if (nx < 1 || ny < 1 || nz < 1 || doubles < 1) throw PspError(kLogicError, "grid sizes must be positive");
 }
@@ -155,11 +171,18 @@ void EnsureDir(const std::string& dir) {
 
 }  // namespace
 
-void GridLoad(const std::string& filename, int nx, int ny, int nz, int doubles, int order, double* d_out) {
+void GridLoad(const std::string& filename, int nx, int ny, int nz, int doubles, int order, double* out) {
     CheckSizes(nx, ny, nz, doubles);
     if (order < kXYZ || order > kZYX) throw PspError(kLogicError, "invalid grid data order");
-    if (!d_out) throw PspError(kLogicError, "null output grid");
+    if (!out) throw PspError(kLogicError, "null output grid");
     const size_t count = (size_t)nx * ny * nz * doubles;
+    if (!OnDevice(out)) {  // host output: through a device buffer
+        DeviceDoubles d(count);
+        GridLoad(filename, nx, ny, nz, doubles, order, d.p);
+        CUDA_CHECK(cudaMemcpy(out, d.p, count * sizeof(double), cudaMemcpyDeviceToHost));
+        return;
+    }
+    double* d_out = out;
     std::vector<double> host(count);
     FILE* f = std::fopen(filename.c_str(), "rb");
     if (!f) throw PspError(kLogicError, "Could not open " + filename);
@@ -188,6 +211,14 @@ void GridInterpolate(const double* d_in, int nxOld, int nyOld, int nzOld, int do
     CheckSizes(nx, ny, nz, doubles);
     if (!d_in || !d_out) throw PspError(kLogicError, "null grid");
     const size_t count = (size_t)nx * ny * nz * doubles;
+    if (!OnDevice(d_in) || !OnDevice(d_out)) {  // host grids: through device buffers
+        const size_t countOld = (size_t)nxOld * nyOld * nzOld * doubles;
+        DeviceDoubles in(countOld), outBuf(count);
+        CUDA_CHECK(cudaMemcpy(in.p, d_in, countOld * sizeof(double), cudaMemcpyDefault));
+        GridInterpolate(in.p, nxOld, nyOld, nzOld, doubles, outBuf.p, nx, ny, nz);
+        CUDA_CHECK(cudaMemcpy(d_out, outBuf.p, count * sizeof(double), cudaMemcpyDefault));
+        return;
+    }
     if (nx == nxOld && ny == nyOld && nz == nzOld) {
         CUDA_CHECK(cudaMemcpy(d_out, d_in, count * sizeof(double), cudaMemcpyDeviceToDevice));
         return;

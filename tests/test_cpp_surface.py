@@ -33,3 +33,43 @@ def test_driver_solves_on_gpu(driver):
         r = subprocess.run([driver, "30", "15", prec], capture_output=True, text=True)
         assert r.returncode == 0, r.stdout + r.stderr
         assert "converged 1" in r.stdout
+
+
+GRID_SRC = os.path.join(ROOT, "tests", "drivers", "grid_io.cpp")
+
+
+@pytest.fixture(scope="module")
+def grid_driver(product_lib, tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("grid") / "grid_io")
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    libdir = os.path.join(ROOT, "psp_b200")
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), GRID_SRC, "-o", out,
+                    "-L", libdir, "-lpsp_b200", "-Wl,-rpath," + libdir], check=True)
+    return out
+
+
+def _driver_grid():
+    import numpy as np
+    z, y, x = np.meshgrid(np.arange(4), np.arange(5), np.arange(6), indexing="ij")
+    return (1.0 + 0.25 * x - 0.5 * y + 0.125 * x * z + 0.01 * y * y)[..., None]
+
+
+def test_grid_writers_from_cpp(grid_driver, tmp_path):
+    from oracle import grid_io as O
+    r = subprocess.run([grid_driver, "write", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    g = _driver_grid()
+    for suffix, text in O.plane_text(g, O.XY, 1).items():
+        assert open(str(tmp_path / "plane") + suffix + ".vti").read() == text
+    for name, text in O.volume_texts(g, str(tmp_path / "volume")).items():
+        assert open(name).read() == text
+
+
+@pytest.mark.gpu
+def test_grid_load_and_resample_from_cpp(grid_driver, tmp_path):
+    import numpy as np
+    from oracle import grid_io as O
+    r = subprocess.run([grid_driver, "load", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = np.fromfile(str(tmp_path / "resampled.bin"), dtype=np.float64).reshape(7, 9, 11, 1)
+    assert np.array_equal(got, O.interpolate_to(_driver_grid(), 11, 9, 7))
