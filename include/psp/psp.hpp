@@ -176,10 +176,29 @@ public:
     }
 
     // Solves in place: the numScalars right-hand sides of B become solutions.
-    psp_cu_stats Solve(DistUniformGrid<C>& B, int m = 20, R relTol = 1e-4, bool /*viewIterates*/ = false) const {
+    // viewIterates writes the iterate of every inner step that does not
+    // converge as iterates-<it> with WriteVolume (solve.hpp:579-585).
+    psp_cu_stats Solve(DistUniformGrid<C>& B, int m = 20, R relTol = 1e-4, bool viewIterates = false) const {
         psp_cu_stats st;
-        detail::Check(psp_cu_solve(h_, reinterpret_cast<double*>(B.Buffer()), B.NumScalars(), m, relTol, &st));
+        if (viewIterates) detail::Check(psp_cu_set_view_iterates(h_, "iterates"));
+        const int e = psp_cu_solve(h_, reinterpret_cast<double*>(B.Buffer()), B.NumScalars(), m, relTol, &st);
+        if (viewIterates) psp_cu_set_view_iterates(h_, nullptr);
+        detail::Check(e);
         return st;
+    }
+
+    // The reference's PRINT_RITZ_VALUES build option as a run-time switch
+    // (0 off, 1 record, 2 record and print), and the recorded Ritz values of
+    // the first restart cycle of the last Solve: right-hand side r's at
+    // [r * count + s], count = the cycle's inner steps.
+    void SetRitzValues(int mode) { detail::Check(psp_cu_set_ritz_values(h_, mode)); }
+    std::vector<C> RitzValues(int* count = nullptr) const {
+        int c = 0, k = 0;
+        detail::Check(psp_cu_get_ritz_values(h_, &c, &k, nullptr));
+        std::vector<C> out((size_t)c * k);
+        if (!out.empty()) detail::Check(psp_cu_get_ritz_values(h_, &c, &k, reinterpret_cast<double*>(out.data())));
+        if (count) *count = c;
+        return out;
     }
     psp_cu_stats SolveWithGMRES(DistUniformGrid<C>& B, int m = 20, R relTol = 1e-4) const {
         return Solve(B, m, relTol);

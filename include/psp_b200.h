@@ -149,6 +149,34 @@ int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel);
 /* Cap on GMRES inner steps (0 = none, the reference behaviour). */
 int psp_cu_set_max_iterations(psp_cu_handle* h, int max_iterations);
 
+/* viewIterates of Solve (solve.hpp:579-585): with a basename, every GMRES
+ * inner step that does not converge writes the current iterate with
+ * WriteVolume (psp_cu_grid_write_volume) as <basename>-<it>, it counting
+ * the inner steps from 0 across restarts (the reference's basename is
+ * "iterates", relative to the working directory).  NULL turns it off. */
+int psp_cu_set_view_iterates(psp_cu_handle* h, const char* basename);
+
+/* The PRINT_RITZ_VALUES build option of the reference (solve.hpp:257-261,
+ * 391-395, 422-426, 589-608) as a run-time mode: 0 off, 1 record the
+ * eigenvalues of the Hessenberg matrix of the first GMRES restart cycle of
+ * each right-hand side at every Solve, 2 record them and print them to
+ * stdout in the reference's format.  LOGIC_ERROR for other modes. */
+int psp_cu_set_ritz_values(psp_cu_handle* h, int mode);
+
+/* The Ritz values of the last Solve that recorded them: *count per
+ * right-hand side (the inner steps of its first restart cycle; 0 if none
+ * were recorded) and *num_rhs; out (may be NULL) receives count*num_rhs
+ * complex values, those of right-hand side r at out[2*(r*count + s)]. */
+int psp_cu_get_ritz_values(const psp_cu_handle* h, int* count, int* num_rhs, double* out);
+
+/* Host only: the eigenvalues of an n x n complex upper Hessenberg matrix H
+ * (column-major, leading dimension ldh, entries below the first subdiagonal
+ * ignored) into w (2n doubles), as Elemental's lapack::HessenbergEig (LAPACK
+ * zhseqr, eigenvalues only) at solve.hpp:597-598 returns them.  LOGIC_ERROR
+ * for bad sizes, RUNTIME_ERROR if the QR iteration does not converge or H
+ * has a non-finite entry. */
+int psp_cu_hessenberg_eigenvalues(int n, const double* H, int ldh, double* w);
+
 /* Panel geometry: number of panels and, if info != NULL, 4 ints per panel
  * (lowest v, depth, padding, class) as in main.hpp:728-821. */
 int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info);

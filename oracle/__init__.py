@@ -186,6 +186,23 @@ class Oracle:
         return X, stats
 
 
+def first_cycle_hessenberg(orc):
+    """The unrotated Hessenberg matrices of the first GMRES restart cycle of
+    the last ``orc.solve`` (the reference's HListCopy, solve.hpp:257-261,
+    391-395, 422-426): complex array (k, count, count), whose eigenvalues
+    are the Ritz values solve.hpp:589-608 prints."""
+    L = lib()
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.oracle_first_cycle_hessenberg.argtypes = [ctypes.c_void_p, ip, ip, ip, ctypes.POINTER(ctypes.c_double)]
+    count, m, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    L.oracle_first_cycle_hessenberg(orc._h, ctypes.byref(count), ctypes.byref(m), ctypes.byref(k), None)
+    H = np.zeros((k.value, m.value, m.value), dtype=np.complex128)  # [r][col][row]
+    L.oracle_first_cycle_hessenberg(orc._h, ctypes.byref(count), ctypes.byref(m), ctypes.byref(k),
+                                    _ptr(H.view(np.float64)))
+    c = count.value
+    return np.ascontiguousarray(H.transpose(0, 2, 1)[:, :c, :c])
+
+
 def sample_costs(orc, velocity, k, reps=2):
     """Bounded timing sample of one workload (see oracle_sample in
     psp_oracle.cpp): dict of seconds per unit of work."""

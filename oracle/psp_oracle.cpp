@@ -90,6 +90,11 @@ struct Solver {
     PanelTree trees[3];
     std::vector<std::vector<Front>> fronts;  // per panel
     bool initialized = false;
+    // HListCopy of the last solve (solve.hpp:257-261, 391-395, 422-426):
+    // the unrotated first-cycle Hessenberg matrices, m x m column-major per
+    // right-hand side, and the cycle's inner-step count.
+    std::vector<C> firstH;
+    int firstCount = 0, firstM = 0, firstK = 0;
 };
 
 // ---------------------------------------------------------------- geometry
@@ -941,6 +946,11 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
         bool converged = false;
         stats->lucky_breakdown = 0;
         double maxRel = 0;
+        bool firstBatch = true;
+        S.firstH.assign((size_t)m * m * k, C(0));
+        S.firstCount = 0;
+        S.firstM = m;
+        S.firstK = k;
         while (!converged) {
             x0 = x;
             Precondition(S, w.data(), k);
@@ -959,6 +969,8 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
                     const C* vi = &V[(size_t)i * n * k];
                     InnerProducts(vi, w.data(), n, k, alpha.data());
                     for (int r = 0; r < k; ++r) H[(size_t)r * m * m + (size_t)j * m + i] = alpha[r];
+                    if (firstBatch)
+                        for (int r = 0; r < k; ++r) S.firstH[(size_t)r * m * m + (size_t)j * m + i] = alpha[r];
                     for (int r = 0; r < k; ++r) {
                         const C a = alpha[r];
                         C* wr = w.data() + (size_t)r * n;
@@ -982,10 +994,13 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
                     stats->final_max_rel_resid = maxRel;
                     return 0;
                 }
-                if (j + 1 != m)
+                if (j + 1 != m) {
                     for (int r = 0; r < k; ++r)
                         for (int q = 0; q < n; ++q)
                             V[(size_t)(j + 1) * n * k + (size_t)r * n + q] = w[(size_t)r * n + q] / delta[r];
+                    if (firstBatch)
+                        for (int r = 0; r < k; ++r) S.firstH[(size_t)r * m * m + (size_t)j * m + j + 1] = delta[r];
+                }
                 for (int r = 0; r < k; ++r) {
                     C* Hr = &H[(size_t)r * m * m];  // column-major m x m, H(i,j) = Hr[j*m+i]
                     for (int i = 0; i < j; ++i) {
@@ -1038,6 +1053,7 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
                 for (int r = 0; r < k; ++r) maxRel = std::max(maxRel, resid[r] / origResid[r]);
                 if (resid_history && it < max_history) resid_history[it] = maxRel;
                 ++it;
+                if (firstBatch) S.firstCount = it;
                 if (maxRel < relTol) {
                     converged = true;
                     break;
@@ -1050,6 +1066,7 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
                     return 0;
                 }
             }
+            firstBatch = false;
         }
         Push(S, (C*)grid, k, x);
         stats->iterations = it;
@@ -1060,6 +1077,20 @@ int oracle_solve(void* h, double* grid, int k, int m, double relTol, int maxIts,
         g_err = e.what();
         return 1;
     }
+}
+
+// The first-cycle Hessenberg matrices of the last oracle_solve (the
+// reference's HListCopy under PRINT_RITZ_VALUES, solve.hpp:589-608): *count
+// inner steps, *m and *k; out (may be null) receives k blocks of m x m
+// complex column-major values.  The Ritz values are the eigenvalues of the
+// leading count x count block of each.
+int oracle_first_cycle_hessenberg(void* h, int* count, int* m, int* k, double* out) {
+    Solver& S = *(Solver*)h;
+    *count = S.firstCount;
+    *m = S.firstM;
+    *k = S.firstK;
+    if (out && !S.firstH.empty()) std::memcpy(out, S.firstH.data(), S.firstH.size() * sizeof(C));
+    return 0;
 }
 
 // Bounded timing sample of the full-size workload for the CPU baseline:

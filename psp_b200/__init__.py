@@ -74,6 +74,7 @@ C_ABI_SYMBOLS = [
     "psp_cu_set_profiling", "psp_cu_profile_reset", "psp_cu_profile_get", "psp_cu_sweep_cost",
     "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device", "psp_cu_initialize_batch", "psp_cu_solve_batch",
     "psp_cu_grid_load", "psp_cu_grid_interpolate", "psp_cu_grid_write_plane", "psp_cu_grid_write_volume",
+    "psp_cu_set_view_iterates", "psp_cu_set_ritz_values", "psp_cu_get_ritz_values", "psp_cu_hessenberg_eigenvalues",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -127,6 +128,10 @@ def lib():
         L.psp_cu_grid_interpolate.argtypes = [vp, ci, ci, ci, ci, ci, vp, ci, ci, ci]
         L.psp_cu_grid_write_plane.argtypes = [dp, ci, ci, ci, ci, ci, ci, ci, ctypes.c_char_p]
         L.psp_cu_grid_write_volume.argtypes = [dp, ci, ci, ci, ci, ci, ctypes.c_char_p]
+        L.psp_cu_set_view_iterates.argtypes = [vp, ctypes.c_char_p]
+        L.psp_cu_set_ritz_values.argtypes = [vp, ci]
+        L.psp_cu_get_ritz_values.argtypes = [vp, ip, ip, dp]
+        L.psp_cu_hessenberg_eigenvalues.argtypes = [ci, dp, ci, dp]
         _lib = L
     return _lib
 
@@ -264,6 +269,20 @@ class DistUniformGrid:
                                               int(self._is_complex()), str(basename).encode()))
 
 
+def hessenberg_eigenvalues(H):
+    """Eigenvalues of a complex upper Hessenberg matrix (entries below the
+    first subdiagonal ignored), as Elemental's lapack::HessenbergEig returns
+    them for the Ritz values of solve.hpp:597-598.  Host only."""
+    A = np.asfortranarray(np.asarray(H, dtype=np.complex128))
+    if A.ndim != 2 or A.shape[0] != A.shape[1]:
+        raise LogicError("Hessenberg matrix must be square")
+    n = A.shape[0]
+    w = np.zeros(n, dtype=np.complex128)
+    _check(lib().psp_cu_hessenberg_eigenvalues(n, _dptr(A.reshape(-1, order="F").view(np.float64)), max(n, 1),
+                                               _dptr(w.view(np.float64))))
+    return w
+
+
 def analyze_class(disc, planes_per_panel=4, cutoff=12, cls=0):
     """Host-only symbolic analysis of one panel class: returns (info, ndToNat)
     with info rows (ND offset, pivot count, update count, parent)."""
@@ -371,7 +390,20 @@ class DistHelmholtz:
     def Solve(self, B, m=20, relTol=1e-4, viewIterates=False):
         """Solve in place (solve.hpp:12-56).  ``B`` is a complex DistUniformGrid
         whose numScalars right-hand sides are replaced by the solutions, or a
-        CUDA complex128 torch tensor of nx*ny*nz*k entries."""
+        CUDA complex128 torch tensor of nx*ny*nz*k entries.  ``viewIterates``
+        (True, or a basename in place of the reference's "iterates") writes
+        the iterate of every inner step that does not converge with
+        WriteVolume as <basename>-<it> (solve.hpp:579-585)."""
+        if not viewIterates:
+            return self._solve(B, m, relTol)
+        base = "iterates" if viewIterates is True else os.fspath(viewIterates)
+        _check(lib().psp_cu_set_view_iterates(self._h, base.encode()))
+        try:
+            return self._solve(B, m, relTol)
+        finally:
+            lib().psp_cu_set_view_iterates(self._h, None)
+
+    def _solve(self, B, m, relTol):
         if _is_cuda_tensor(B):
             k = B.numel() // self.N
             st = _Stats()
@@ -398,6 +430,23 @@ class DistHelmholtz:
 
     def set_max_iterations(self, n):
         _check(lib().psp_cu_set_max_iterations(self._h, int(n)))
+
+    def SetRitzValues(self, mode):
+        """PRINT_RITZ_VALUES (solve.hpp:589-608) at run time: 0 off, 1 record
+        the Ritz values of the first GMRES restart cycle of every Solve, 2
+        record and print them as the reference does."""
+        _check(lib().psp_cu_set_ritz_values(self._h, int(mode)))
+
+    def RitzValues(self):
+        """Ritz values of the last Solve that recorded them: complex array
+        (numRhs, steps of the first restart cycle)."""
+        count, k = ctypes.c_int(), ctypes.c_int()
+        _check(lib().psp_cu_get_ritz_values(self._h, ctypes.byref(count), ctypes.byref(k), None))
+        out = np.zeros(count.value * k.value, dtype=np.complex128)
+        if out.size:
+            _check(lib().psp_cu_get_ritz_values(self._h, ctypes.byref(count), ctypes.byref(k),
+                                                _dptr(out.view(np.float64))))
+        return out.reshape(k.value, count.value)
 
     def setup_info(self):
         s = ctypes.c_double()

@@ -7,6 +7,7 @@
 #include "../../include/psp_b200.h"
 #include "grid_io.hpp"
 #include "handle.hpp"
+#include "ritz.hpp"
 #include "solver.hpp"
 
 using psp_b200::Helmholtz;
@@ -226,6 +227,39 @@ int psp_cu_set_max_iterations(psp_cu_handle* h, int max_iterations) {
     if (int e = CheckHandle(h)) return e;
     h->solver->SetMaxIterations(max_iterations);
     return PSP_CU_OK;
+}
+
+int psp_cu_set_view_iterates(psp_cu_handle* h, const char* basename) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->SetViewIterates(basename ? std::string(basename) : std::string()); });
+}
+
+int psp_cu_set_ritz_values(psp_cu_handle* h, int mode) {
+    if (int e = CheckHandle(h)) return e;
+    if (mode < 0 || mode > 2) {
+        g_lastError = "Ritz value mode must be 0, 1 or 2";
+        return PSP_CU_LOGIC_ERROR;
+    }
+    h->solver->SetRitzValues(mode);
+    return PSP_CU_OK;
+}
+
+int psp_cu_get_ritz_values(const psp_cu_handle* h, int* count, int* num_rhs, double* out) {
+    if (int e = CheckHandle(h)) return e;
+    const Helmholtz& s = *h->solver;
+    if (count) *count = s.ritzCount();
+    if (num_rhs) *num_rhs = s.ritzNumRhs();
+    if (out && !s.ritzValues().empty())
+        std::memcpy(out, s.ritzValues().data(), s.ritzValues().size() * sizeof(std::complex<double>));
+    return PSP_CU_OK;
+}
+
+int psp_cu_hessenberg_eigenvalues(int n, const double* H, int ldh, double* w) {
+    return Guard([&] {
+        if (n > 0 && !w) throw std::logic_error("eigenvalue output is null");
+        const auto ev = psp_b200::HessenbergEigenvalues(n, reinterpret_cast<const std::complex<double>*>(H), ldh);
+        if (n > 0) std::memcpy(w, ev.data(), ev.size() * sizeof(std::complex<double>));
+    });
 }
 
 int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info) {

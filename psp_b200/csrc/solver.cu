@@ -7,9 +7,14 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <iostream>
+#include <string>
 #include <type_traits>
 
 #include "solver.hpp"
+
+#include "grid_io.hpp"
+#include "ritz.hpp"
 
 namespace psp_b200 {
 
@@ -1178,6 +1183,36 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
 
     std::vector<Cd> H((size_t)k * m * m), z((size_t)k * (m + 1)), sn((size_t)k * m), y((size_t)m * k), hcol;
     std::vector<double> cs((size_t)k * m);
+    // HListCopy of solve.hpp:257-261: the unrotated Hessenberg matrices of
+    // the first restart cycle, one m x m column-major block per RHS.
+    ritz_.clear();
+    ritzCount_ = ritzK_ = 0;
+    bool firstBatch = ritzMode_ > 0;
+    std::vector<Cd> Hfirst(firstBatch ? (size_t)k * m * m : 0, Cd(0));
+    auto ritzValues = [&](int count) {
+        ritzCount_ = count;
+        ritzK_ = k;
+        ritz_.assign((size_t)k * count, Cd(0));
+        for (int r = 0; r < k; ++r) {
+            const std::vector<Cd> ev = HessenbergEigenvalues(count, &Hfirst[(size_t)r * m * m], m);
+            std::copy(ev.begin(), ev.end(), ritz_.begin() + (size_t)r * count);
+            if (ritzMode_ > 1) {
+                std::cout << "Ritz values for " << r << "'th right-hand side before first restart:\n";
+                for (int q = 0; q < count; ++q) std::cout << ev[q] << " ";
+                std::cout << std::endl;
+            }
+        }
+    };
+    // viewIterates (solve.hpp:579-585): the current iterate in the grid's
+    // natural [N][k] layout, written with WriteVolume.
+    std::vector<z64> xHost;
+    auto writeIterate = [&](int step) {
+        xHost.resize(nk);
+        CUDA_CHECK(cudaMemcpyAsync(xHost.data(), x, nk * sizeof(z64), cudaMemcpyDeviceToHost, st));
+        CUDA_CHECK(cudaStreamSynchronize(st));
+        GridWriteVolume(reinterpret_cast<const double*>(xHost.data()), an_.disc.nx, an_.disc.ny, an_.disc.nz, k,
+                        true, viewIterates_ + "-" + std::to_string(step));
+    };
     int it = 0;
     bool converged = false;
     double maxRel = 0;
@@ -1220,6 +1255,12 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
                 S.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
                 return;
             }
+            if (firstBatch)
+                for (int r = 0; r < k; ++r) {
+                    Cd* Hr = &Hfirst[(size_t)r * m * m];
+                    for (int i = 0; i <= j; ++i) Hr[(size_t)j * m + i] = Cd(hcol[(size_t)i * k + r]);
+                    if (j + 1 != m) Hr[(size_t)j * m + j + 1] = delta[r];
+                }
             phases.Begin(st);
             if (j + 1 != m) LaunchScaleColumns(w, dDelta, V + (size_t)(j + 1) * nk, N, k, st);
             for (int r = 0; r < k; ++r) {
@@ -1263,13 +1304,19 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
             maxRel = 0;
             for (int r = 0; r < k; ++r) maxRel = std::max(maxRel, resid[r] / origResid[r]);
             S.history.push_back(maxRel);
-            ++it;
             if (maxRel < relTol) {
                 converged = true;
+                ++it;
                 break;
             }
+            if (!viewIterates_.empty()) writeIterate(it);
+            ++it;
             if (maxIterations_ > 0 && it >= maxIterations_) break;
         }
+        // solve.hpp:589-608: after the first restart cycle, `it` is its
+        // number of inner steps.
+        if (firstBatch) ritzValues(it);
+        firstBatch = false;
         if (maxIterations_ > 0 && it >= maxIterations_) break;
     }
     CUDA_CHECK(cudaMemcpyAsync(B, x, nk * sizeof(z64), cudaMemcpyDeviceToDevice, st));

@@ -4,6 +4,7 @@
 #include <complex>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "analysis.hpp"
@@ -96,6 +97,19 @@ public:
     double setupSeconds() const { return setupSeconds_; }
     int64_t factorBytes() const;
     void SetMaxIterations(int n) { maxIterations_ = n; }
+    // viewIterates (solve.hpp:579-585): a non-empty basename makes every
+    // GMRES inner step that does not converge write the iterate with
+    // WriteVolume as <basename>-<it>.
+    void SetViewIterates(const std::string& basename) { viewIterates_ = basename; }
+    // PRINT_RITZ_VALUES (solve.hpp:257-261, 391-395, 422-426, 589-608) at
+    // run time: 0 off, 1 record the Ritz values of the first restart cycle
+    // of each Solve, 2 record and print them as the reference does.
+    void SetRitzValues(int mode) { ritzMode_ = mode; }
+    // Ritz values of the last Solve that recorded them: ritzCount() per
+    // right-hand side, right-hand side r at [r * ritzCount() + s].
+    const std::vector<std::complex<double>>& ritzValues() const { return ritz_; }
+    int ritzCount() const { return ritzCount_; }
+    int ritzNumRhs() const { return ritzK_; }
     Profiler& profiler() { return prof_; }
     // Sweep algorithmic flops/bytes for k right-hand sides (0 before Initialize).
     double SweepFlops(int k) const;
@@ -123,6 +137,9 @@ private:
     bool initialized_ = false;
     int precision_ = 0;
     int maxIterations_ = 0;
+    std::string viewIterates_;
+    int ritzMode_ = 0, ritzCount_ = 0, ritzK_ = 0;
+    std::vector<std::complex<double>> ritz_;
     double setupSeconds_ = 0;
     std::unique_ptr<FactorStore<double>> f64_;
     std::unique_ptr<FactorStore<float>> f32_;

@@ -3,7 +3,11 @@
 // style of the reference's tests/UnitCube.cpp: a converging-lens velocity,
 // Gaussian point sources, timed Initialize and Solve.
 //
-//   unit_cube [n] [omega] [precision 0|1] [m] [relTol]
+//   unit_cube [n] [omega] [precision 0|1] [m] [relTol] [diagnostics]
+//
+// diagnostics: bit 0 solves with viewIterates (iterates-<it> volumes in the
+// working directory), bit 1 prints the first-cycle Ritz values as the
+// reference's PRINT_RITZ_VALUES build does.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -19,6 +23,7 @@ int main(int argc, char** argv) {
     const Precision prec = (argc > 3 && std::atoi(argv[3]) == 1) ? MIXED : FP64;
     const int m = argc > 4 ? std::atoi(argv[4]) : 20;
     const double relTol = argc > 5 ? std::atof(argv[5]) : 1e-5;
+    const int diagnostics = argc > 6 ? std::atoi(argv[6]) : 0;
     try {
         Discretization<double> disc(omega, n, n, n, 1., 1., 1., PML, PML, PML, PML, PML, 5, 1.5);
         DistHelmholtz<double> helmholtz(disc);
@@ -49,8 +54,9 @@ int main(int argc, char** argv) {
                     b[i + 0] = -n * std::exp(-10. * n * a0);
                     b[i + 1] = -n * std::exp(-10. * n * a1);
                 }
+        if (diagnostics & 2) helmholtz.SetRitzValues(2);
         const auto t1 = std::chrono::steady_clock::now();
-        const psp_cu_stats st = helmholtz.Solve(B, m, relTol);
+        const psp_cu_stats st = helmholtz.Solve(B, m, relTol, (diagnostics & 1) != 0);
         const double tSolve = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
         double norm = 0;
         for (int i = 0; i < n * n * n * k; ++i) norm += std::norm(b[i]);

@@ -73,3 +73,22 @@ def test_grid_load_and_resample_from_cpp(grid_driver, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     got = np.fromfile(str(tmp_path / "resampled.bin"), dtype=np.float64).reshape(7, 9, 11, 1)
     assert np.array_equal(got, O.interpolate_to(_driver_grid(), 11, 9, 7))
+
+
+@pytest.mark.gpu
+def test_driver_diagnostics(driver, tmp_path):
+    # viewIterates and the Ritz-value printout through psp.hpp
+    r = subprocess.run([driver, "30", "15", "0", "20", "1e-5", "3"], capture_output=True, text=True,
+                       cwd=str(tmp_path))
+    assert r.returncode == 0, r.stdout + r.stderr
+    its = int(r.stdout.split("iterations ")[1].split()[0])
+    for it in range(its - 1):
+        for rhs in range(2):
+            for part in ("real", "imag"):
+                stem = tmp_path / ("iterates-%d_%d_%s" % (it, rhs, part))
+                assert (tmp_path / (stem.name + ".pvti")).exists() and (stem / "0.vti").exists()
+    assert not (tmp_path / ("iterates-%d_0_real.pvti" % (its - 1))).exists()
+    lines = r.stdout.splitlines()
+    for rhs in range(2):
+        i = lines.index("Ritz values for %d'th right-hand side before first restart:" % rhs)
+        assert len(lines[i + 1].split()) == min(its, 20)
