@@ -5,9 +5,12 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
+#include <map>
+#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -43,6 +46,13 @@ void TaskArena::Upload(cudaStream_t st) {
 namespace {
 
 typedef std::complex<double> Cd;
+
+// Sweep variants (kernel and K-chunk per depth) chosen by timing, shared by
+// every handle of the process with the same front structure, block width
+// and device: equal problems then run the same kernels (a re-initialized handle and a fresh
+// one give identical results) and a batch of equal problems is timed once.
+std::mutex gRouteMutex;
+std::map<std::string, std::vector<int>> gRoutes;
 
 // Imaginary stretch of a PML point at distance `delta` from the inner edge
 // (the common body of s1Inv/s2Inv/s3Inv/s3InvArtificial,
@@ -208,12 +218,27 @@ private:
     std::vector<int64_t> gOff_, dOff_;
     std::vector<std::vector<int>> depthNodes_;
     DeviceBuffer status_;
+    // One way to run the solve GEMM of one depth and direction: the kernel
+    // (tensor cores, tiles of kTcRows rows; or CUDA cores, kSweepRows rows)
+    // and the K-chunk of its tiles.
+    struct SweepVariant {
+        bool tc = false;
+        int chunk = 0;
+        size_t tiles = 0;  // arena offset of the tile list
+        int n = 0;
+    };
+    // Per tree depth and direction: the candidate variants and the one in
+    // use (complex single: chosen by timing them all, Autotune).
     struct ClassPlan {
         size_t pre = 0;
         int preN = 0;
-        std::vector<size_t> fTiles, bTiles, bGather;
-        std::vector<int> fN, bN, bGatherN, fChunk, bChunk;
+        std::vector<size_t> bGather;
+        std::vector<int> bGatherN;
+        std::vector<std::vector<SweepVariant>> fVar, bVar;
+        std::vector<int> fSel, bSel;
         std::vector<double> fFlops, fBytes, bFlops, bBytes;
+        const SweepVariant& F(int d) const { return fVar[d][fSel[d]]; }
+        const SweepVariant& B(int d) const { return bVar[d][bSel[d]]; }
     };
     // Task lists and work vectors of the panel solves for one RHS block width.
     // Plans live as long as the factors: captured sweep graphs point into them.
@@ -230,11 +255,23 @@ private:
     };
     std::vector<std::unique_ptr<SolvePlan>> plans_;
     SolvePlan& Plan(int k);
+    // Times every candidate variant of every depth of one panel solve per
+    // class (scratch right-hand sides) and keeps the fastest per depth and
+    // direction.  Events bracket each solve-GEMM launch while tune_ is set.
+    void Autotune(SolvePlan& P);
+    struct TuneEvents {
+        std::vector<cudaEvent_t> ev;
+        int used = 0;
+    };
+    TuneEvents* tune_ = nullptr;
+    void TuneMark() {
+        if (tune_ && tune_->used < (int)tune_->ev.size())
+            CUDA_CHECK(cudaEventRecord(tune_->ev[tune_->used++], h_.stream_));
+    }
     bool tc_ = false;  // tensor-core sweep kernels (complex single only)
     bool factorTc_ = false;  // tensor-core factorization GEMMs (complex single only)
     // Ops of at least this many rows and K columns take tensor-core tiles.
     bool UseGemmTc(const GemmOp<R>& op) const { return factorTc_ && op.M >= 64 && op.K >= 16; }
-    int TileRows() const { return tc_ ? kTcRows : kSweepRows; }
 };
 
 template <typename R>
@@ -660,14 +697,15 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // has a few CTAs per SM; rows of a tile share one K range (inv(L11) is
     // triangular, so the forward range stops at the tile's last row and the
     // backward range starts at its first).
-    // The tensor-core kernels are persistent and pipeline across tiles, so
-    // long chunks cost nothing extra and save split-K partial sums; the
-    // chunk only shrinks to give every SM tiles.
-    const int maxChunk = tc_ ? 512 : SweepMaxChunk<R>();
-    const int tileRows = TileRows();
-    int64_t maxSlots = 1, maxCounters = 1;
-    auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepTile>& tiles, int& chunk,
-                         double& flops, double& bytes) {
+    // The default chunk starts at the kernel's longest (the tensor-core
+    // kernels are persistent and pipeline across tiles, so long chunks cost
+    // nothing extra and save split-K partial sums) and only shrinks to give
+    // every SM tiles; `forceChunk` > 0 fixes it instead (tuning candidates).
+    int64_t maxPartialRows = kTcRows, maxCounters = 1;
+    auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, bool tcTiles, int forceChunk,
+                         std::vector<SweepTile>& tiles) {
+        const int maxChunk = tcTiles ? 512 : SweepMaxChunk<R>();
+        const int tileRows = tcTiles ? kTcRows : kSweepRows;
         auto build = [&](int kc, bool emit) {
             int64_t n = 0, slots = 0, counters = 0;
             for (int t : depthNodes_[d]) {
@@ -695,19 +733,21 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
                     }
             }
             if (emit) {
-                maxSlots = std::max(maxSlots, slots);
+                maxPartialRows = std::max(maxPartialRows, slots * tileRows);
                 maxCounters = std::max(maxCounters, counters);
             }
             return n;
         };
-        int kc = maxChunk;
-        while (kc > 64 && build(kc, false) < 2 * 148) kc /= 2;
+        int kc = forceChunk > 0 ? forceChunk : maxChunk;
+        while (forceChunk <= 0 && kc > 64 && build(kc, false) < 2 * 148) kc /= 2;
         build(kc, true);
-        chunk = kc;
         // longest K ranges first, so the launch does not end on a long tail
         std::stable_sort(tiles.begin(), tiles.end(), [](const SweepTile& a, const SweepTile& b) {
             return (a.k1 - a.k0) > (b.k1 - b.k0);
         });
+        return kc;
+    };
+    auto depthCost = [&](const ClassStructure& cs, int d, bool fwd, double& flops, double& bytes) {
         for (int t : depthNodes_[d]) {
             const double s = cs.size[t], u = cs.usize[t];
             const double nz = (s + u) * s - s * (s - 1) / 2;  // nonzeros of G
@@ -715,42 +755,202 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             bytes += sizeof(cpx<R>) * (nz + (fwd ? (s + 2 * (s + u)) : (2 * (s + u) + 2 * s)) * k);
         }
     };
+    // Candidates of one depth and direction: the default tiling of each
+    // kernel and, with tensor cores, the other chunk lengths (a tiling equal
+    // to an earlier candidate's is skipped).
+    auto makeVariants = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepVariant>& out) {
+        std::vector<std::pair<bool, int>> cand;
+        if (tc_) {
+            cand.push_back({true, 0});
+            for (int kc : {64, 128, 256, 512}) cand.push_back({true, kc});
+            cand.push_back({false, 0});
+            for (int kc : {64, 128}) cand.push_back({false, kc});
+        } else {
+            cand.push_back({false, 0});
+        }
+        std::vector<std::vector<SweepTile>> seen;
+        for (const auto& cd : cand) {
+            std::vector<SweepTile> tiles;
+            SweepVariant v;
+            v.tc = cd.first;
+            v.chunk = makeTiles(cs, d, fwd, cd.first, cd.second, tiles);
+            bool dup = false;
+            for (size_t i = 0; i < seen.size() && !dup; ++i)
+                dup = out[i].tc == v.tc && seen[i].size() == tiles.size() &&
+                      std::equal(tiles.begin(), tiles.end(), seen[i].begin(), [](const SweepTile& a, const SweepTile& b) {
+                          return a.front == b.front && a.row0 == b.row0 && a.col0 == b.col0 && a.k0 == b.k0 &&
+                                 a.k1 == b.k1;
+                      });
+            if (dup) continue;
+            v.tiles = P.arena.Push(tiles);
+            v.n = (int)tiles.size();
+            out.push_back(v);
+            seen.push_back(std::move(tiles));
+        }
+    };
     for (int c = 0; c < 3; ++c) {
         if (!an_.classUsed[c]) continue;
         const ClassStructure& cs = an_.cls[c];
         ClassPlan& cp = P.cplan[c];
-        cp.fTiles.assign(nd, 0); cp.bTiles.assign(nd, 0); cp.bGather.assign(nd, 0);
-        cp.fN.assign(nd, 0); cp.bN.assign(nd, 0); cp.bGatherN.assign(nd, 0);
-        cp.fChunk.assign(nd, 0); cp.bChunk.assign(nd, 0);
+        cp.bGather.assign(nd, 0);
+        cp.bGatherN.assign(nd, 0);
+        cp.fVar.assign(nd, {});
+        cp.bVar.assign(nd, {});
+        cp.fSel.assign(nd, 0);
+        cp.bSel.assign(nd, 0);
         cp.fFlops.assign(nd, 0); cp.fBytes.assign(nd, 0); cp.bFlops.assign(nd, 0); cp.bBytes.assign(nd, 0);
         std::vector<int2> pre;
         for (int d = 0; d < nd; ++d) {
-            std::vector<SweepTile> ft, bt;
             std::vector<int2> bg;
-            makeTiles(cs, d, true, ft, cp.fChunk[d], cp.fFlops[d], cp.fBytes[d]);
-            makeTiles(cs, d, false, bt, cp.bChunk[d], cp.bFlops[d], cp.bBytes[d]);
+            makeVariants(cs, d, true, cp.fVar[d]);
+            makeVariants(cs, d, false, cp.bVar[d]);
+            depthCost(cs, d, true, cp.fFlops[d], cp.fBytes[d]);
+            depthCost(cs, d, false, cp.bFlops[d], cp.bBytes[d]);
             for (int t : depthNodes_[d])
                 for (int i0 = 0; i0 < cs.size[t] + cs.usize[t]; i0 += kSweepRows) {
                     bg.push_back(make_int2(t, i0));
                     pre.push_back(make_int2(t, i0));
                 }
-            cp.fTiles[d] = P.arena.Push(ft);
-            cp.fN[d] = (int)ft.size();
-            cp.bTiles[d] = P.arena.Push(bt);
-            cp.bN[d] = (int)bt.size();
             cp.bGather[d] = P.arena.Push(bg);
             cp.bGatherN[d] = (int)bg.size();
         }
         cp.pre = P.arena.Push(pre);
         cp.preN = (int)pre.size();
     }
-    P.partials.Allocate((size_t)maxSlots * tileRows * kSweepCols * sizeof(cpx<R>));
+    P.partials.Allocate((size_t)maxPartialRows * kSweepCols * sizeof(cpx<R>));
     P.counters.Allocate((size_t)maxCounters * sizeof(int));
     CUDA_CHECK(cudaMemsetAsync(P.counters.p, 0, P.counters.bytes, h_.stream_));
     P.arena.Upload(h_.stream_);
-    if (tc_)
+    if (tc_) {
         CUDA_CHECK(cudaMemcpyAsync(P.maps.p, P.mapsHost.data(), P.maps.bytes, cudaMemcpyHostToDevice, h_.stream_));
+        // PSP_B200_SWEEP_AUTOTUNE: unset = time every candidate per depth;
+        // "0" = the default tensor-core tiling everywhere; "alternate" = a
+        // fixed mix of tensor-core and CUDA-core depths (tests).
+        const char* env = std::getenv("PSP_B200_SWEEP_AUTOTUNE");
+        const std::string mode = env ? env : "";
+        if (mode == "alternate") {
+            for (ClassPlan& cp : P.cplan)
+                for (size_t d = 0; d < cp.fVar.size(); ++d) {
+                    auto firstOf = [](const std::vector<SweepVariant>& vs, bool tc) {
+                        for (size_t i = 0; i < vs.size(); ++i)
+                            if (vs[i].tc == tc) return (int)i;
+                        return 0;
+                    };
+                    cp.fSel[d] = firstOf(cp.fVar[d], d % 2 == 1);
+                    cp.bSel[d] = firstOf(cp.bVar[d], d % 2 == 0);
+                }
+        } else if (mode != "0") {
+            std::string key = std::to_string(k) + "/" + std::to_string(h_.device());
+            for (int c = 0; c < 3; ++c) {
+                if (!an_.classUsed[c]) continue;
+                const ClassStructure& cs = an_.cls[c];
+                key += "|" + std::to_string(c) + ":";
+                for (size_t t = 0; t < cs.size.size(); ++t)
+                    key += std::to_string(cs.size[t]) + "," + std::to_string(cs.usize[t]) + ";";
+            }
+            std::vector<int> routes;
+            {
+                std::lock_guard<std::mutex> lock(gRouteMutex);
+                auto it = gRoutes.find(key);
+                if (it != gRoutes.end()) routes = it->second;
+            }
+            if (routes.empty()) {
+                Autotune(P);
+                for (const ClassPlan& cp : P.cplan) {
+                    routes.insert(routes.end(), cp.fSel.begin(), cp.fSel.end());
+                    routes.insert(routes.end(), cp.bSel.begin(), cp.bSel.end());
+                }
+                std::lock_guard<std::mutex> lock(gRouteMutex);
+                gRoutes.emplace(key, routes);
+            } else {
+                size_t i = 0;
+                for (ClassPlan& cp : P.cplan) {
+                    for (int& r : cp.fSel) r = routes[i++];
+                    for (int& r : cp.bSel) r = routes[i++];
+                }
+            }
+        }
+    }
     return P;
+}
+
+template <typename R>
+void FactorStore<R>::Autotune(SolvePlan& P) {
+    const PanelGeometry& g = an_.geom;
+    const int nd = (int)depthNodes_.size(), k = P.k;
+    const int reps = 3;
+    DeviceBuffer scratch;
+    scratch.Allocate((size_t)h_.NumUnknowns() * k * sizeof(z64));
+    CUDA_CHECK(cudaMemsetAsync(scratch.p, 0, scratch.bytes, h_.stream_));
+    TuneEvents te;
+    te.ev.resize(4 * nd);
+    for (cudaEvent_t& e : te.ev) CUDA_CHECK(cudaEventCreate(&e));
+    const char* verbose = std::getenv("PSP_B200_SWEEP_AUTOTUNE_VERBOSE");
+    const bool talk = verbose && verbose[0] == '1';
+    try {
+        for (int c = 0; c < 3; ++c) {
+            int p = -1;
+            for (int q = 0; q < g.numPanels && p < 0; ++q)
+                if (g.Class(q) == c) p = q;
+            if (p < 0) continue;
+            ClassPlan& cp = P.cplan[c];
+            size_t maxVar = 0;
+            for (int d = 0; d < nd; ++d) maxVar = std::max({maxVar, cp.fVar[d].size(), cp.bVar[d].size()});
+            // [direction][depth][variant] best milliseconds
+            std::vector<std::vector<float>> best[2];
+            for (int dir = 0; dir < 2; ++dir) {
+                best[dir].assign(nd, {});
+                for (int d = 0; d < nd; ++d) best[dir][d].assign((dir ? cp.bVar : cp.fVar)[d].size(), 1e30f);
+            }
+            // run v times every depth's v-th candidate (its first where it has fewer)
+            for (size_t v = 0; v < maxVar; ++v) {
+                for (int d = 0; d < nd; ++d) {
+                    cp.fSel[d] = v < cp.fVar[d].size() ? (int)v : 0;
+                    cp.bSel[d] = v < cp.bVar[d].size() ? (int)v : 0;
+                }
+                for (int rep = 0; rep <= reps; ++rep) {
+                    te.used = 0;
+                    tune_ = &te;
+                    SolvePanel(scratch.as<z64>(), k, k, p, 0, 0);
+                    tune_ = nullptr;
+                    CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
+                    if (rep == 0 || te.used != 4 * nd) continue;  // the first run warms up
+                    for (int i = 0; i < nd; ++i) {
+                        float fms = 0, bms = 0;
+                        CUDA_CHECK(cudaEventElapsedTime(&fms, te.ev[2 * i], te.ev[2 * i + 1]));
+                        CUDA_CHECK(cudaEventElapsedTime(&bms, te.ev[2 * nd + 2 * i], te.ev[2 * nd + 2 * i + 1]));
+                        const int df = nd - 1 - i;  // the forward walks the depths bottom-up
+                        float& bf = best[0][df][cp.fSel[df]];
+                        float& bb = best[1][i][cp.bSel[i]];
+                        bf = std::min(bf, fms);
+                        bb = std::min(bb, bms);
+                    }
+                }
+            }
+            for (int d = 0; d < nd; ++d) {
+                for (int dir = 0; dir < 2; ++dir) {
+                    const std::vector<float>& b = best[dir][d];
+                    (dir ? cp.bSel : cp.fSel)[d] = (int)(std::min_element(b.begin(), b.end()) - b.begin());
+                }
+                if (talk) {
+                    std::fprintf(stderr, "sweep autotune k=%d class %d depth %2d:", k, c, d);
+                    for (int dir = 0; dir < 2; ++dir) {
+                        const std::vector<SweepVariant>& vs = (dir ? cp.bVar : cp.fVar)[d];
+                        std::fprintf(stderr, dir ? "  bwd" : " fwd");
+                        for (size_t i = 0; i < vs.size(); ++i)
+                            std::fprintf(stderr, " %s%s%d %.4f", (int)i == (dir ? cp.bSel : cp.fSel)[d] ? "*" : "",
+                                         vs[i].tc ? "tc" : "cc", vs[i].chunk, best[dir][d][i]);
+                    }
+                    std::fprintf(stderr, "\n");
+                }
+            }
+        }
+    } catch (...) {
+        tune_ = nullptr;
+        for (cudaEvent_t e : te.ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (cudaEvent_t e : te.ev) CUDA_CHECK(cudaEventDestroy(e));
 }
 
 template <typename R>
@@ -786,29 +986,38 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     }
     for (int d = nd - 1; d >= 0; --d) {
         ProfScope ps(st, kProfSolveGemm, cp.fFlops[d], cp.fBytes[d]);
-        const SweepTile* tl = P.arena.template At<SweepTile>(cp.fTiles[d]);
+        const SweepVariant& v = cp.F(d);
+        const SweepTile* tl = P.arena.template At<SweepTile>(v.tiles);
+        TuneMark();
+        bool done = false;
         if constexpr (std::is_same<R, float>::value) {
-            if (tc_) {
-                LaunchSweepForwardTc(fr, tl, cp.fN[d], k, w, st);
-                continue;
+            if (v.tc) {
+                LaunchSweepForwardTc(fr, tl, v.n, k, w, st);
+                done = true;
             }
         }
-        LaunchSweepForward<R>(fr, tl, cp.fN[d], cp.fChunk[d], k, w, st);
+        if (!done) LaunchSweepForward<R>(fr, tl, v.n, v.chunk, k, w, st);
+        TuneMark();
     }
     for (int d = 0; d < nd; ++d) {
         {
             ProfScope ps(st, kProfGatherScatter);
-            LaunchSweepBackwardGather<R>(fr, P.arena.template At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st, tc_);
+            LaunchSweepBackwardGather<R>(fr, P.arena.template At<int2>(cp.bGather[d]), cp.bGatherN[d], k, w, st,
+                                         cp.B(d).tc);
         }
         ProfScope ps(st, kProfSolveGemm, cp.bFlops[d], cp.bBytes[d]);
-        const SweepTile* tl = P.arena.template At<SweepTile>(cp.bTiles[d]);
+        const SweepVariant& v = cp.B(d);
+        const SweepTile* tl = P.arena.template At<SweepTile>(v.tiles);
+        TuneMark();
+        bool done = false;
         if constexpr (std::is_same<R, float>::value) {
-            if (tc_) {
-                LaunchSweepBackwardTc(fr, tl, cp.bN[d], B, k, io, w, st);
-                continue;
+            if (v.tc) {
+                LaunchSweepBackwardTc(fr, tl, v.n, B, k, io, w, st);
+                done = true;
             }
         }
-        LaunchSweepBackward<R>(fr, tl, cp.bN[d], cp.bChunk[d], B, k, io, w, st);
+        if (!done) LaunchSweepBackward<R>(fr, tl, v.n, v.chunk, B, k, io, w, st);
+        TuneMark();
     }
 }
 
