@@ -738,8 +738,12 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             }
             return n;
         };
+        // default: shrink until the launch has tiles for every SM (CUDA-core
+        // CTAs, two per SM) or for half of them (persistent tensor-core CTAs,
+        // whose long K pipelines beat extra split-K partial sums)
+        const int64_t minTiles = tcTiles ? 74 : 2 * 148;
         int kc = forceChunk > 0 ? forceChunk : maxChunk;
-        while (forceChunk <= 0 && kc > 64 && build(kc, false) < 2 * 148) kc /= 2;
+        while (forceChunk <= 0 && kc > 64 && build(kc, false) < minTiles) kc /= 2;
         build(kc, true);
         // longest K ranges first, so the launch does not end on a long tail
         std::stable_sort(tiles.begin(), tiles.end(), [](const SweepTile& a, const SweepTile& b) {
@@ -823,11 +827,15 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     P.arena.Upload(h_.stream_);
     if (tc_) {
         CUDA_CHECK(cudaMemcpyAsync(P.maps.p, P.mapsHost.data(), P.maps.bytes, cudaMemcpyHostToDevice, h_.stream_));
-        // PSP_B200_SWEEP_AUTOTUNE: unset = time every candidate per depth;
-        // "0" = the default tensor-core tiling everywhere; "alternate" = a
-        // fixed mix of tensor-core and CUDA-core depths (tests).
+        // PSP_B200_SWEEP_AUTOTUNE: unset = time every candidate per depth on
+        // problems of at least 2^20 unknowns (where the timing, a few sweeps'
+        // worth, is small against a solve), else the default tiling; "1" =
+        // time them at any size; "0" = the default tensor-core tiling
+        // everywhere; "alternate" = a fixed mix of tensor-core and CUDA-core
+        // depths (tests).
         const char* env = std::getenv("PSP_B200_SWEEP_AUTOTUNE");
-        const std::string mode = env ? env : "";
+        std::string mode = env ? env : "";
+        if (mode.empty()) mode = h_.NumUnknowns() >= (int64_t(1) << 20) ? "1" : "0";
         if (mode == "alternate") {
             for (ClassPlan& cp : P.cplan)
                 for (size_t d = 0; d < cp.fVar.size(); ++d) {
@@ -839,7 +847,7 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
                     cp.fSel[d] = firstOf(cp.fVar[d], d % 2 == 1);
                     cp.bSel[d] = firstOf(cp.bVar[d], d % 2 == 0);
                 }
-        } else if (mode != "0") {
+        } else if (mode == "1") {
             std::string key = std::to_string(k) + "/" + std::to_string(h_.device());
             for (int c = 0; c < 3; ++c) {
                 if (!an_.classUsed[c]) continue;
@@ -878,7 +886,7 @@ template <typename R>
 void FactorStore<R>::Autotune(SolvePlan& P) {
     const PanelGeometry& g = an_.geom;
     const int nd = (int)depthNodes_.size(), k = P.k;
-    const int reps = 3;
+    const int reps = 2;
     DeviceBuffer scratch;
     scratch.Allocate((size_t)h_.NumUnknowns() * k * sizeof(z64));
     CUDA_CHECK(cudaMemsetAsync(scratch.p, 0, scratch.bytes, h_.stream_));

@@ -1,8 +1,9 @@
 """Per-depth choice between the tensor-core and the CUDA-core sweep kernels
 (complex single).
 
-The sweep plan times every tree depth of one panel solve per panel class on
-both kernels and keeps the faster for each depth and direction.  Both
+The sweep plan times every candidate (kernel and K-chunk) of every tree
+depth of one panel solve per panel class and keeps the fastest for each
+depth and direction.  Both
 kernels read and write the same front work vectors, so any mix must give
 the same preconditioner up to single-precision rounding: a fixed
 alternating mix, tensor cores everywhere, CUDA cores everywhere and the
@@ -55,7 +56,7 @@ def setup(product_lib):
     O = oracle_for(w.disc)
     O.initialize(w.velocity)
     routes = {
-        "auto": {"PSP_B200_SWEEP_AUTOTUNE": None, "PSP_B200_SWEEP_CUDA_CORES": None},
+        "auto": {"PSP_B200_SWEEP_AUTOTUNE": "1", "PSP_B200_SWEEP_CUDA_CORES": None},
         "tensor": {"PSP_B200_SWEEP_AUTOTUNE": "0", "PSP_B200_SWEEP_CUDA_CORES": None},
         "alternate": {"PSP_B200_SWEEP_AUTOTUNE": "alternate", "PSP_B200_SWEEP_CUDA_CORES": None},
         "cuda_cores": {"PSP_B200_SWEEP_AUTOTUNE": None, "PSP_B200_SWEEP_CUDA_CORES": "1"},
