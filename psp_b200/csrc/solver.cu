@@ -693,10 +693,9 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
         }
         P.panelFronts[p] = P.arena.Push(fr);
     }
-    // Tiles of one depth and direction.  The K-chunk shrinks until the launch
-    // has a few CTAs per SM; rows of a tile share one K range (inv(L11) is
-    // triangular, so the forward range stops at the tile's last row and the
-    // backward range starts at its first).
+    // Tiles of one depth and direction: rows of a tile share one K range
+    // (inv(L11) is triangular, so the forward range stops at the tile's last
+    // row and the backward range starts at its first), split into chunks.
     // The default chunk starts at the kernel's longest (the tensor-core
     // kernels are persistent and pipeline across tiles, so long chunks cost
     // nothing extra and save split-K partial sums) and only shrinks to give
