@@ -34,6 +34,12 @@ def test_null_arguments_are_logic_errors(product_lib):
     assert product_lib.psp_cu_create(None, 7.0, 4, 12, 0, ctypes.byref(h)) == 1
     assert b"null" in product_lib.psp_cu_last_error()
     assert product_lib.psp_cu_finalize(None) == 1
+    # the diagnostics switches and their read-out check the handle too
+    assert product_lib.psp_cu_set_view_iterates(None, b"iterates") == 1
+    assert product_lib.psp_cu_set_ritz_values(None, 1) == 1
+    count, k = ctypes.c_int(-1), ctypes.c_int(-1)
+    assert product_lib.psp_cu_get_ritz_values(None, ctypes.byref(count), ctypes.byref(k), None) == 1
+    assert count.value == -1 and k.value == -1
 
 
 def test_compute_without_device_fails_loudly(product_lib):
