@@ -256,8 +256,9 @@ private:
     std::vector<std::unique_ptr<SolvePlan>> plans_;
     SolvePlan& Plan(int k);
     // Times every candidate variant of every depth of one panel solve per
-    // class (scratch right-hand sides) and keeps the fastest per depth and
-    // direction.  Events bracket each solve-GEMM launch while tune_ is set.
+    // class (scratch right-hand sides; without room for them the default
+    // tiling stays) and keeps the fastest per depth and direction.  Events
+    // bracket each solve-GEMM launch while tune_ is set.
     void Autotune(SolvePlan& P);
     struct TuneEvents {
         std::vector<cudaEvent_t> ev;
@@ -887,7 +888,13 @@ void FactorStore<R>::Autotune(SolvePlan& P) {
     const int nd = (int)depthNodes_.size(), k = P.k;
     const int reps = 2;
     DeviceBuffer scratch;
-    scratch.Allocate((size_t)h_.NumUnknowns() * k * sizeof(z64));
+    try {
+        scratch.Allocate((size_t)h_.NumUnknowns() * k * sizeof(z64));
+    } catch (const PspError& e) {
+        if (e.code != kOutOfMemory) throw;
+        cudaGetLastError();  // no room for timing runs: keep the default tiling
+        return;
+    }
     CUDA_CHECK(cudaMemsetAsync(scratch.p, 0, scratch.bytes, h_.stream_));
     TuneEvents te;
     te.ev.resize(4 * nd);
