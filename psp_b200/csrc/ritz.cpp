@@ -24,8 +24,9 @@ void Rotation(Cd f, Cd g, double& c, Cd& s) {
 }  // namespace
 
 // Explicitly shifted QR iteration on the unreduced trailing window [l, hi]
-// of the Hessenberg matrix (Golub & Van Loan, Matrix Computations, 4th ed.,
-// 7.5): H - mu I = QR by Givens rotations, H := RQ + mu I.  The shift is the
+// of the Hessenberg matrix, scaled by a power of two to unit size (Golub &
+// Van Loan, Matrix Computations, 4th ed., 7.5): H - mu I = QR by Givens
+// rotations, H := RQ + mu I.  The shift is the
 // eigenvalue of the trailing 2x2 block closer to its last diagonal entry
 // (Wilkinson), replaced by an ad hoc shift after 10 and 20 sweeps without a
 // deflation.  A subdiagonal entry deflates when it is below the unit
@@ -38,9 +39,17 @@ std::vector<Cd> HessenbergEigenvalues(int n, const Cd* H, int ldh) {
     for (int j = 0; j < n; ++j)
         for (int i = 0; i <= std::min(j + 1, n - 1); ++i) A[(size_t)j * n + i] = H[(size_t)j * ldh + i];
     auto a = [&](int i, int j) -> Cd& { return A[(size_t)j * n + i]; };
-    for (const Cd& v : A)
+    double amax = 0;
+    for (const Cd& v : A) {
         if (!std::isfinite(v.real()) || !std::isfinite(v.imag()))
             throw std::runtime_error("Hessenberg matrix has a non-finite entry");
+        amax = std::max({amax, std::abs(v.real()), std::abs(v.imag())});
+    }
+    // Work on H / 2^e with the largest entry near 1 (exact: a power of two),
+    // so that the shifts' products neither overflow nor underflow.
+    const int e = amax > 0 ? std::ilogb(amax) : 0;
+    if (e != 0)
+        for (Cd& v : A) v = Cd(std::ldexp(v.real(), -e), std::ldexp(v.imag(), -e));
 
     std::vector<Cd> w(n);
     std::vector<double> cs(n);
@@ -102,6 +111,8 @@ std::vector<Cd> HessenbergEigenvalues(int n, const Cd* H, int ldh) {
         }
         for (int i = l; i <= hi; ++i) a(i, i) += mu;
     }
+    if (e != 0)
+        for (Cd& v : w) v = Cd(std::ldexp(v.real(), e), std::ldexp(v.imag(), e));
     return w;
 }
 

@@ -65,6 +65,21 @@ def test_hessenberg_eigenvalues_special_matrices(product_lib):
     assert match_error(P.hessenberg_eigenvalues(B), np.linalg.eigvals(B)) < 1e-12
 
 
+def test_hessenberg_eigenvalues_at_extreme_scales(product_lib):
+    # the routine works on H scaled by a power of two, so the eigenvalues of
+    # 2^e H are exactly 2^e times those of H, far beyond where unscaled
+    # shift products would overflow or underflow
+    rng = np.random.default_rng(11)
+    H = np.triu(rng.standard_normal((17, 17)) + 1j * rng.standard_normal((17, 17)), -1)
+    w = P.hessenberg_eigenvalues(H)
+    for e in (-900, -600, 600, 900):
+        assert np.array_equal(P.hessenberg_eigenvalues(H * 2.0 ** e), w * 2.0 ** e), e
+    # tiny subdiagonal entries beside unit-size ones deflate
+    T = np.triu(rng.standard_normal((6, 6)) + 0j, -1)
+    T[3, 2] = 1e-300
+    assert match_error(P.hessenberg_eigenvalues(T), np.linalg.eigvals(T)) < 1e-12
+
+
 def test_hessenberg_eigenvalues_errors(product_lib):
     import ctypes
     H = np.zeros(8)
