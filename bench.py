@@ -265,6 +265,10 @@ def gradient_arm(args, ws, local):
     return out
 
 
+# problems in flight per rank in the batch arm (one handle and stream each)
+BATCH_STREAMS = 4
+
+
 def batch_arm(args, ws, rank, local):
     """Throughput over the batching workload: 48 independent problems (sides
     32-96, k = 1-8) split over the ranks by predicted cost (longest
@@ -282,14 +286,15 @@ def batch_arm(args, ws, rank, local):
     barrier(ws)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    _, rep = B.solve_batch(probs, RESTART, REL_TOL, P.MIXED, rank, ws, local, gather=False, costs=costs)
+    _, rep = B.solve_batch(probs, RESTART, REL_TOL, P.MIXED, rank, ws, local, gather=False, costs=costs,
+                           streams=BATCH_STREAMS)
     torch.cuda.synchronize()
     sec = max_over_ranks(time.perf_counter() - t0, ws)
     total_k = sum(p.k for p in probs)
     return {"value": total_k / sec, "unit": "RHS/s", "seconds": sec, "problems": len(probs), "rhs": total_k,
             "workload": "batch_48", "precision": "mixed", "scaling": "strong (fixed batch over ranks)",
             "predicted_loads_s": [round(x, 4) for x in loads],
-            "problems_per_rank": [len(b) for b in bins],
+            "problems_per_rank": [len(b) for b in bins], "streams_per_rank": BATCH_STREAMS,
             "timing": "host wall clock around the rank's share, max over ranks (many short solves)"}
 
 

@@ -13,8 +13,13 @@ device within 4/3 of the optimum.
 ``solve_batch`` runs this rank's share.  With ``world > 1`` it is called by
 every rank of an initialized ``torch.distributed`` process group (NCCL on
 GPUs, gloo on CPU), and the solutions are exchanged with all_gather_object.
+With ``streams > 1`` a rank keeps that many problems in flight at once, each
+on its own handle and CUDA stream (host threads; the library's calls release
+the interpreter lock), so the launches of small problems, which leave most
+SMs idle, overlap on the GPU.
 """
 import math
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -77,7 +82,7 @@ def _gpu_solver(problem, device, precision):
 
 
 def solve_batch(problems, m=20, rel_tol=1e-4, precision=MIXED, rank=0, world=1, device=0, gather=True,
-                costs=None, make_solver=None):
+                costs=None, make_solver=None, streams=1):
     """Solves this rank's share of ``problems`` (LPT over ``world`` ranks).
 
     Returns (solutions, report): ``solutions`` maps problem index to
@@ -85,20 +90,28 @@ def solve_batch(problems, m=20, rel_tol=1e-4, precision=MIXED, rank=0, world=1, 
     ``gather`` and world > 1; ``report`` holds the assignment and predicted
     loads.  ``make_solver(problem, device, precision)`` returns an
     initialized object with ``Solve(X, m, rel_tol)`` and ``Finalize()``
-    (default: a DistHelmholtz on ``device``)."""
+    (default: a DistHelmholtz on ``device``).  ``streams``: problems in
+    flight at once on this rank, taken in decreasing predicted cost; each
+    result is the same as with one stream."""
     if costs is None:
         costs = [predicted_cost(p.disc, p.k) for p in problems]
     bins, loads = lpt_assign(costs, world)
     make_solver = make_solver or _gpu_solver
-    mine = {}
-    for i in bins[rank]:
+
+    def run(i):
         p = problems[i]
         H = make_solver(p, device, precision)
         X = np.ascontiguousarray(p.rhs, dtype=np.complex128).copy()
         st = H.Solve(X, m, rel_tol)
         H.Finalize()
-        mine[i] = (X, st)
-    report = {"bins": bins, "predicted_loads": loads, "rank": rank, "world": world}
+        return i, (X, st)
+
+    if streams > 1 and len(bins[rank]) > 1:
+        with ThreadPoolExecutor(max_workers=streams) as ex:
+            mine = dict(ex.map(run, bins[rank]))
+    else:
+        mine = dict(run(i) for i in bins[rank])
+    report = {"bins": bins, "predicted_loads": loads, "rank": rank, "world": world, "streams": streams}
     if world > 1 and gather:
         import torch.distributed as dist
         parts = [None] * world
