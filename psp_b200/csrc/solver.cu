@@ -51,7 +51,7 @@ typedef std::complex<double> Cd;
 // every handle of the process with the same front structure, block width
 // and device: equal problems then run the same kernels (a re-initialized handle and a fresh
 // one give identical results) and a batch of equal problems is timed once.
-std::mutex gRouteMutex;
+std::mutex gRouteMutex, gTuneMutex;
 std::map<std::string, std::vector<int>> gRoutes;
 
 // Imaginary stretch of a PML point at distance `delta` from the inner edge
@@ -857,25 +857,32 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
                     key += std::to_string(cs.size[t]) + "," + std::to_string(cs.usize[t]) + ";";
             }
             std::vector<int> routes;
-            {
+            auto lookup = [&] {
                 std::lock_guard<std::mutex> lock(gRouteMutex);
                 auto it = gRoutes.find(key);
                 if (it != gRoutes.end()) routes = it->second;
-            }
+            };
+            lookup();
             if (routes.empty()) {
-                Autotune(P);
-                for (const ClassPlan& cp : P.cplan) {
-                    routes.insert(routes.end(), cp.fSel.begin(), cp.fSel.end());
-                    routes.insert(routes.end(), cp.bSel.begin(), cp.bSel.end());
+                // one tuning run at a time in the process: a handle with the
+                // same structure waits for it and reuses its choices, and
+                // no two tuning runs time each other's launches
+                std::lock_guard<std::mutex> tuning(gTuneMutex);
+                lookup();
+                if (routes.empty()) {
+                    Autotune(P);
+                    for (const ClassPlan& cp : P.cplan) {
+                        routes.insert(routes.end(), cp.fSel.begin(), cp.fSel.end());
+                        routes.insert(routes.end(), cp.bSel.begin(), cp.bSel.end());
+                    }
+                    std::lock_guard<std::mutex> lock(gRouteMutex);
+                    gRoutes.emplace(key, routes);
                 }
-                std::lock_guard<std::mutex> lock(gRouteMutex);
-                gRoutes.emplace(key, routes);
-            } else {
-                size_t i = 0;
-                for (ClassPlan& cp : P.cplan) {
-                    for (int& r : cp.fSel) r = routes[i++];
-                    for (int& r : cp.bSel) r = routes[i++];
-                }
+            }
+            size_t i = 0;
+            for (ClassPlan& cp : P.cplan) {
+                for (int& r : cp.fSel) r = routes[i++];
+                for (int& r : cp.bSel) r = routes[i++];
             }
         }
     }
