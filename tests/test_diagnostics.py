@@ -134,6 +134,13 @@ def test_oracle_first_cycle_hessenberg_is_arnoldi():
     # a cycle that converges early records only its steps
     _, st = O.solve(b, m=20, rel_tol=1e-3)
     assert oracle.first_cycle_hessenberg(O).shape == (w.k, st["iterations"], st["iterations"])
+    # with restarts only the first cycle is kept: its m steps, whose last
+    # subdiagonal entry (outside the m x m block) is never stored
+    _, st = O.solve(b, m=3, rel_tol=1e-6)
+    assert st["iterations"] > 3
+    H3 = oracle.first_cycle_hessenberg(O)
+    assert H3.shape == (w.k, 3, 3)
+    assert np.abs(H3 - want[:, :3, :3]).max() <= 1e-9 * np.abs(want).max()
 
 
 # ---------------------------------------------------------------- GPU
