@@ -98,7 +98,11 @@ int psp_cu_solve_batch(psp_cu_handle* const* h, double* const* B, const int* k, 
                        psp_cu_stats* stats, int* failed);
 
 /* DistHelmholtz::Solve(B, m, relTol) (include/psp/dist_helmholtz/solve.hpp:12-56):
- * B is a host grid of nx*ny*nz*k complex values, overwritten by the solution. */
+ * B is a host grid of nx*ny*nz*k complex values, overwritten by the solution.
+ * When the GMRES workspace of all k right-hand sides (about nx*ny*nz*k*(m+5)
+ * complex doubles) does not fit in device memory, blocks of right-hand sides
+ * are solved one after another, each to the tolerance; stats then report the
+ * largest step count and residual over the blocks. */
 int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_cu_stats* stats);
 
 /* The same on a device grid owned by the caller. */

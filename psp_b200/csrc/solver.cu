@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -1355,7 +1356,91 @@ bool AnyNaN(const std::vector<double>& v) {
 
 }  // namespace
 
+int Helmholtz::GmresBlockWidth(int k, int m) {
+    int kb = k;
+    if (const char* env = std::getenv("PSP_B200_MAX_RHS_BLOCK")) {
+        const int cap = std::atoi(env);
+        if (cap > 0) kb = std::min(kb, cap);
+    }
+    size_t freeB = 0, totalB = 0;
+    CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
+    // the workspace held now is released before a different width is allocated
+    const double held = wsK_ > 0 ? (double)NumUnknowns() * wsK_ * sizeof(z64) * (wsM_ + 4) : 0.0;
+    // V (m vectors), x, x0, w, b and a block's copy of its columns
+    const double perRhs = (double)NumUnknowns() * sizeof(z64) * (m + 6);
+    const double fit = std::floor(0.85 * ((double)freeB + held) / perRhs);
+    if (fit >= 1 && fit < kb) kb = (int)fit;
+    return std::max(1, kb);
+}
+
 void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* stats) {
+    if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    if (k < 1) throw PspError(kLogicError, "need at least one right-hand side");
+    if (m < 1) throw PspError(kLogicError, "GMRES restart length must be positive");
+    CUDA_CHECK(cudaSetDevice(device_));
+    const int kb = GmresBlockWidth(k, m);
+    if (kb >= k) {
+        SolveBlock(B, k, m, relTol, stats);
+        return;
+    }
+    const auto tStart = std::chrono::steady_clock::now();
+    SolveStats local;
+    SolveStats& S = stats ? *stats : local;
+    S = SolveStats();
+    S.converged = 1;
+    const int64_t N = NumUnknowns();
+    DeviceBuffer cols;
+    cols.Allocate((size_t)N * kb * sizeof(z64));
+    const std::string viewBase = viewIterates_;
+    std::vector<std::vector<Cd>> ritzPerRhs;
+    int ritzCount = 0;
+    struct Restore {
+        Helmholtz& h;
+        std::string base;
+        ~Restore() { h.viewIterates_ = base; h.ritzRhsOffset_ = 0; }
+    } restore{*this, viewBase};
+    for (int c0 = 0; c0 < k; c0 += kb) {
+        const int w = std::min(kb, k - c0);
+        // columns [c0, c0 + w) of the [N][k] grid as a contiguous [N][w] grid
+        CUDA_CHECK(cudaMemcpy2DAsync(cols.p, w * sizeof(z64), B + c0, k * sizeof(z64), w * sizeof(z64), N,
+                                     cudaMemcpyDeviceToDevice, stream_));
+        if (!viewBase.empty()) viewIterates_ = viewBase + "_rhs" + std::to_string(c0);
+        ritzRhsOffset_ = c0;
+        SolveStats s;
+        SolveBlock(cols.as<z64>(), w, m, relTol, &s);
+        CUDA_CHECK(cudaMemcpy2DAsync(B + c0, k * sizeof(z64), cols.p, w * sizeof(z64), w * sizeof(z64), N,
+                                     cudaMemcpyDeviceToDevice, stream_));
+        S.iterations = std::max(S.iterations, s.iterations);
+        S.converged = S.converged && s.converged;
+        S.luckyBreakdown = S.luckyBreakdown || s.luckyBreakdown;
+        S.finalMaxRelResid = std::max(S.finalMaxRelResid, s.finalMaxRelResid);
+        S.precondSeconds += s.precondSeconds;
+        S.matvecSeconds += s.matvecSeconds;
+        S.arnoldiSeconds += s.arnoldiSeconds;
+        S.numPreconditions += s.numPreconditions;
+        if (S.history.size() < s.history.size()) S.history.resize(s.history.size(), 0.0);
+        for (size_t i = 0; i < s.history.size(); ++i) S.history[i] = std::max(S.history[i], s.history[i]);
+        if (ritzK_ > 0) {
+            for (int r = 0; r < ritzK_; ++r)
+                ritzPerRhs.emplace_back(ritz_.begin() + (size_t)r * ritzCount_,
+                                        ritz_.begin() + (size_t)(r + 1) * ritzCount_);
+            ritzCount = std::max(ritzCount, ritzCount_);
+        }
+    }
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+    ritz_.clear();
+    ritzCount_ = ritzK_ = 0;
+    if ((int)ritzPerRhs.size() == k) {
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        ritz_.assign((size_t)k * ritzCount, Cd(nan, nan));
+        for (int r = 0; r < k; ++r) std::copy(ritzPerRhs[r].begin(), ritzPerRhs[r].end(), ritz_.begin() + (size_t)r * ritzCount);
+        ritzCount_ = ritzCount;
+        ritzK_ = k;
+    }
+    S.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tStart).count();
+}
+
+void Helmholtz::SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stats) {
     if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
     if (k < 1) throw PspError(kLogicError, "need at least one right-hand side");
     if (m < 1) throw PspError(kLogicError, "GMRES restart length must be positive");
@@ -1427,7 +1512,8 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
             const std::vector<Cd> ev = HessenbergEigenvalues(count, &Hfirst[(size_t)r * m * m], m);
             std::copy(ev.begin(), ev.end(), ritz_.begin() + (size_t)r * count);
             if (ritzMode_ > 1) {
-                std::cout << "Ritz values for " << r << "'th right-hand side before first restart:\n";
+                std::cout << "Ritz values for " << ritzRhsOffset_ + r
+                          << "'th right-hand side before first restart:\n";
                 for (int q = 0; q < count; ++q) std::cout << ev[q] << " ";
                 std::cout << std::endl;
             }

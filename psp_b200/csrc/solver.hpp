@@ -80,6 +80,15 @@ public:
     bool Initialized() const { return initialized_; }
 
     // Solve (solve.hpp:12-56) on a device natural-order [N][k] complex grid, in place.
+    // When the GMRES workspace of all k right-hand sides (about N k (m+5)
+    // complex doubles) does not fit in device memory, or the environment
+    // caps the width (PSP_B200_MAX_RHS_BLOCK), the right-hand sides are
+    // solved in blocks one after another: every block converges on its own
+    // (the GMRES of one right-hand side never depends on the others), the
+    // stats report the largest step count and residual, viewIterates files
+    // carry the block's first column (<basename>_rhs<c>-<it>), and Ritz
+    // values of right-hand sides whose first cycle was shorter than the
+    // longest are padded with NaN.
     void SolveDevice(z64* B, int k, int m, double relTol, SolveStats* stats);
     // B := A B and B := M^{-1} B on device grids (Multiply / Precondition).
     void MultiplyDevice(z64* B, int k);
@@ -132,13 +141,17 @@ private:
     void Precondition(z64* B, int k, bool useGraph);
     void EnsureWorkspace(int k, int m);
     void CheckSweepStatus();
+    // GMRES over all k columns of B at once (the reference's form).
+    void SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stats);
+    // Right-hand sides per GMRES block for k sides and restart m.
+    int GmresBlockWidth(int k, int m);
 
     Profiler prof_;
     bool initialized_ = false;
     int precision_ = 0;
     int maxIterations_ = 0;
     std::string viewIterates_;
-    int ritzMode_ = 0, ritzCount_ = 0, ritzK_ = 0;
+    int ritzMode_ = 0, ritzCount_ = 0, ritzK_ = 0, ritzRhsOffset_ = 0;
     std::vector<std::complex<double>> ritz_;
     double setupSeconds_ = 0;
     std::unique_ptr<FactorStore<double>> f64_;
