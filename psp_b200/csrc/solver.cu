@@ -1389,6 +1389,11 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     S = SolveStats();
     S.converged = 1;
     const int64_t N = NumUnknowns();
+    if (wsK_ != kb || wsM_ != m) {
+        // the blocks allocate their own width; free the old one first
+        for (DeviceBuffer* b : {&dX_, &dX0_, &dW_, &dB_, &dV_, &dPartial_, &dScal_, &dY_}) b->Release();
+        wsK_ = wsM_ = -1;
+    }
     DeviceBuffer cols;
     cols.Allocate((size_t)N * kb * sizeof(z64));
     const std::string viewBase = viewIterates_;
