@@ -3,15 +3,24 @@
 
 Metric: Helmholtz solve RHS/s to relative residual 1e-4 (GMRES(20)), mixed
 precision (complex-single fronts and sweeps, FP64 GMRES) next to the plain
-FP64 path.  One step = Initialize(velocity) + Solve of the workload's k
-right-hand sides, i.e. setup and solve of one batch; solve-only RHS/s is
-reported beside it.
+FP64 path; gradients/s beside it.
 
-Workload: the 116^3 smooth-anomaly problem (100^3 interior + 8 PML points per
-face, omega = 2 pi 10, 16 Gaussian sources), seeded synthetic inputs built by
-psp_b200.workloads.
+Workload (default ``large_220``): the 200 x 200 x 100 interior with 10 PML
+points per face (220 x 220 x 120 points, 5.8M unknowns), a 12-layer velocity
+of 1.5-6.0 with three dipping faults and one anticline, omega at 10 points
+per wavelength of the slowest layer, 64 Gaussian sources; seeded synthetic
+inputs built by psp_b200.workloads.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+A step is one Solve of one GMRES block of right-hand sides against factors
+from one Initialize: the 64 sources go through the solver in equal blocks
+as wide as device memory allows next to the complex-single factors (the
+width the library itself picks for a 64-source Solve; 32 on a B200), so a
+64-source job is two steps.  ``value`` is solve-only RHS/s (right-hand
+sides / device time of the Solve calls), the figure the reference's drivers
+report when they time Solve apart from Initialize; Initialize is timed on
+its own and setup+solve RHS/s is reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config NAME]
 
 Under torchrun every rank solves its own copy of the workload (weak scaling,
 no collective on the data path); timing is the max over ranks of the device
@@ -19,6 +28,7 @@ time between CUDA events on the solver's stream.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -37,18 +47,19 @@ REL_TOL = 1e-4
 RESTART = 20
 
 # GMRES(20) inner steps the FP64 path takes to 1e-4 on each workload; the
-# CPU-baseline model multiplies the sampled per-step costs by this count (the
-# FP64 GPU path runs the oracle's algorithm step for step).
+# CPU model multiplies its sampled per-step costs by this count (the FP64 GPU
+# path runs the oracle's algorithm step for step, so its count is the
+# oracle's).  Workloads not listed use the count of the run's own solve.
 FP64_ITERATIONS = {"smooth_anomalies_116": 15, "plain_bump_50": 16}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="smooth_anomalies_116")
+    ap.add_argument("--config", default="large_220")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true")
@@ -189,40 +200,100 @@ def barrier(ws):
     ranks.barrier(ws)
 
 
-def run_arm(H, w, vel_d, rhs_d, X, precision, steps, warmup, ws, stream, clocks=None):
-    """Times `steps` Initialize+Solve steps on the solver stream."""
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        pass
+
+
+def workload(name):
+    from psp_b200 import workloads as W
+    return W.CONFIGS[name]()
+
+
+def config_dict(name, w, kb):
+    """The workload as both arms name it."""
+    return {"workload": name, "grid": [w.disc.nx, w.disc.ny, w.disc.nz], "interior": list(w.interior),
+            "pml": w.pml, "k": w.k, "rhs_per_step": kb, "gmres_restart": RESTART, "rel_tol": REL_TOL,
+            "step": "Solve of one GMRES block of rhs_per_step right-hand sides (factors from one Initialize, "
+                    "timed apart)",
+            "l2": "inputs larger than L2 (factors > 10 GB)", "parallelism": "independent problem per GPU"}
+
+
+# GMRES block width of each workload's mixed-precision solve on one B200
+# (what the library picks for all k sources next to its complex-single
+# factors); the reference arm, which runs without a GPU, names the same
+# block.  Workloads not listed solve all k at once.
+BLOCK_WIDTH = {"large_220": 32}
+
+
+def ev():
     import torch
-    import psp_b200 as P
+    return torch.cuda.Event(enable_timing=True)
 
-    def step(ev):
-        ev[0].record(stream)
+
+def time_initialize(H, vel_d, precision, reps, stream):
+    """Milliseconds of `reps` timed Initialize calls after one untimed one."""
+    H.Initialize(vel_d, precision=precision)
+    ms = []
+    for _ in range(reps):
+        e0, e1 = ev(), ev()
+        e0.record(stream)
         H.Initialize(vel_d, precision=precision)
-        ev[1].record(stream)
-        with torch.cuda.stream(stream):
-            X.copy_(rhs_d)
-        st = H.Solve(X, RESTART, REL_TOL)
-        ev[2].record(stream)
-        return st
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
 
-    for _ in range(warmup):
-        step([torch.cuda.Event(enable_timing=True) for _ in range(3)])
+
+def block_cols(w, kb, i):
+    """Sources of block i (blocks of kb cycle over the k sources)."""
+    nb = -(-w.k // kb)
+    c0 = (i % nb) * kb
+    return range(c0, min(w.k, c0 + kb))
+
+
+def solve_steps(H, w, kb, steps, warmup, ws, stream, clocks=None):
+    """Times `steps` block Solves (after `warmup` untimed ones) with CUDA
+    events on the solver stream; each step's right-hand sides are written on
+    the device before its events."""
+    import torch
+    N = w.disc.nx * w.disc.ny * w.disc.nz
+    X = torch.empty(N * kb, dtype=torch.complex128, device="cuda")
+
+    def step(i, rec):
+        cols = block_cols(w, kb, i)
+        Xv = X[:N * len(cols)]
+        w.rhs_torch("cuda", Xv, cols)
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        st = H.Solve(Xv, RESTART, REL_TOL)
+        e1.record(stream)
+        e1.synchronize()
+        rec.append((e0.elapsed_time(e1), len(cols), st))
+
+    junk = []
+    for i in range(warmup):
+        step(i, junk)
     barrier(ws)
     torch.cuda.synchronize()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
-    stats = []
+    recs = []
     ctx = clocks if clocks is not None else _Null()
     with ctx:
         for i in range(steps):
-            stats.append(step(evs[i]))
+            step(warmup + i, recs)
         torch.cuda.synchronize()
     barrier(ws)
-    setup_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
-    solve_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
-    total_ms = sum(e[0].elapsed_time(e[2]) for e in evs)
-    total_ms = max_over_ranks(total_ms, ws)
-    solve_ms = max_over_ranks(solve_ms, ws)
-    setup_ms = max_over_ranks(setup_ms, ws)
-    return dict(total_ms=total_ms, setup_ms=setup_ms, solve_ms=solve_ms, stats=stats)
+    total_ms = max_over_ranks(sum(r[0] for r in recs), ws)
+    rhs = sum(r[1] for r in recs)
+    return dict(total_ms=total_ms, rhs=rhs, stats=[r[2] for r in recs], X=X)
+
+
+# timed gradients (and warm-up ones) at most, whatever the main arm's steps
+GRAD_STEPS = 5
 
 
 def gradient_arm(args, ws, local):
@@ -245,18 +316,20 @@ def gradient_arm(args, ws, local):
     H.Solve(u_obs, RESTART, REL_TOL)
     data = u_obs[recv].clone()
     del u_obs
-    for _ in range(args.warmup):
+    steps, warmup = min(args.steps, GRAD_STEPS), min(args.warmup, GRAD_STEPS)
+    for _ in range(max(1, warmup)):
         J, g = misfit_and_gradient(H, vel, f, recv, data, RESTART, REL_TOL, P.MIXED)
     barrier(ws)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         J, g = misfit_and_gradient(H, vel, f, recv, data, RESTART, REL_TOL, P.MIXED)
     e1.record()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), ws)
-    out = {"value": ws * args.steps / (ms * 1e-3), "unit": "gradients/s", "ms_per_gradient": ms / args.steps,
+    out = {"value": ws * steps / (ms * 1e-3), "unit": "gradients/s", "ms_per_gradient": ms / steps,
+           "steps": steps,
            "workload": args.grad_config, "grid": [w.disc.nx, w.disc.ny, w.disc.nz], "sources": k,
            "receivers": int(len(w.meta["receivers"])), "precision": "mixed",
            "step": "Initialize + forward solve + adjoint solve + gradient kernel",
@@ -303,55 +376,107 @@ def W_batch():
     return W.batch_problems()
 
 
-class _Null:
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *a):
-        pass
-
-
-def profile_step(H, vel_d, rhs_d, X, precision, stream):
+def fp64_sample(H, w, vel_d, stream, mixed_block0):
+    """The plain FP64 path on the same workload, measured once: one timed
+    Initialize (after an untimed one; panels whose complex-double factors do
+    not fit are recomputed during the sweeps), then one Solve of the first
+    GMRES block the FP64 handle picks for the k sources."""
     import torch
+    import psp_b200 as P
+    setup = time_initialize(H, vel_d, P.FP64, 1, stream)
+    mem = H.memory_info()
+    kb = H.solve_block_width(w.k, RESTART)
+    N = w.disc.nx * w.disc.ny * w.disc.nz
+    cols = range(0, kb)
+    X = w.rhs_torch("cuda", cols=cols)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    st = H.Solve(X, RESTART, REL_TOL)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    refactors = H.memory_info()["refactorizations"]
+    out = {"value": kb / (ms * 1e-3), "unit": UNIT, "rhs": kb, "steps": 1,
+           "solve_ms": ms, "setup_ms": setup[0], "iterations": st["iterations"],
+           "final_rel_resid": st["final_max_rel_resid"], "converged": st["converged"],
+           "resident_panels": mem["resident_panels"], "num_panels": mem["num_panels"],
+           "refactorizations_in_solve": refactors,
+           "setup_plus_solve_rhs_per_s": w.k / ((setup[0] + math.ceil(w.k / kb) * ms) * 1e-3),
+           "note": ("one Solve of the first %d sources; setup+solve counts one Initialize and %d such blocks"
+                    % (kb, math.ceil(w.k / kb)))}
+    if mixed_block0 is not None:
+        n = min(kb, mixed_block0.shape[-1])
+        a = torch.from_numpy(mixed_block0[..., :n].reshape(-1)).cuda()
+        b = X.view(N, kb)[:, :n].reshape(-1)
+        out["mixed_rel_diff_vs_fp64"] = float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    del X
+    return out
+
+
+def e2e_arm(H, w, vel_h, kb, nsteps, ws, stream):
+    """The same metric through the public API with host buffers: each step
+    is one Solve of a block of kb host right-hand sides (numpy), so its
+    host-to-device copy of the sources and device-to-host copy of the
+    wavefields are inside the timed region; Initialize from the host
+    velocity first (timed apart, as in the device-resident arm)."""
+    import torch
+    import psp_b200 as P
+    H.Initialize(vel_h, precision=P.MIXED)
+    blocks = [w.rhs_host(block_cols(w, kb, i)) for i in range(min(nsteps, -(-w.k // kb)))]
+    B = blocks[0].copy()
+    H.Solve(B, RESTART, REL_TOL)  # untimed: the handle's pinned staging and device scratch
+    barrier(ws)
+    torch.cuda.synchronize()
+    ms = 0.0
+    rhs = 0
+    for i in range(nsteps):
+        B = blocks[i % len(blocks)].copy()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        H.Solve(B, RESTART, REL_TOL)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        rhs += B.shape[-1]
+    ms = max_over_ranks(ms, ws)
+    N = w.disc.nx * w.disc.ny * w.disc.nz
+    return {"value": ws * rhs / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(N * kb * 16),
+            "d2h_bytes_per_step": int(N * kb * 16), "steps": nsteps,
+            "path": "psp_cu_solve with host buffers (pinned staging ring, copies inside the timed region)"}
+
+
+def profile_block(H, w, kb, stream):
+    """One block Solve with per-kernel profiling (sweeps eager)."""
+    import torch
+    N = w.disc.nx * w.disc.ny * w.disc.nz
+    X = w.rhs_torch("cuda", cols=block_cols(w, kb, 0))
     H.set_profiling(True)
     H.profile_reset()
-    H.Initialize(vel_d, precision=precision)
-    with torch.cuda.stream(stream):
-        X.copy_(rhs_d)
     H.Solve(X, RESTART, REL_TOL)
     torch.cuda.synchronize()
     prof = H.profile()
     H.set_profiling(False)
+    del X
     return prof
 
 
+# DRAM bytes per algorithmic byte of a sweep launch, from one ncu capture
+# of the forward tensor-core sweep kernel on a profiling-sized member of the
+# workload family (profiles/)
 SWEEP_TRAFFIC_RATIO = (20.43e6 + 2.8e3) / 16.84e6
 
 
-def roofline_from_profile(prof, peaks):
-    kernels = {k: v for k, v in prof.items() if k != "sweep" and v["launches"] > 0}
-    name = max(kernels, key=lambda k: kernels[k]["ms"])
-    p = kernels[name]
+def roofline_entry(name, p, peaks):
     sec = p["ms"] * 1e-3
     ai = p["flops"] / max(p["bytes"], 1.0)
     ridge = peaks["bf16_tflops"] * 1e12 / (peaks["hbm_gbs"] * 1e9)
     if ai > ridge:
-        achieved = p["flops"] / sec / 1e12
-        out = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s"}
+        out = {"bound": "tensor", "achieved": p["flops"] / sec / 1e12, "peak": peaks["bf16_tflops"],
+               "unit": "TFLOP/s"}
     else:
-        achieved = p["bytes"] / sec / 1e9
-        out = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s"}
+        out = {"bound": "hbm", "achieved": p["bytes"] / sec / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s"}
     out["frac"] = out["achieved"] / out["peak"]
-    if name == "solve_gemm":
-        # DRAM bytes per algorithmic byte of a sweep launch, from one ncu
-        # capture of the forward tensor-core sweep kernel on the 56^3 member
-        # of this workload family (depth 6 of the bottom panel: 20.43 MB read
-        # for 16.84 MB algorithmic), applied to this launch's algorithmic bytes
-        out["traffic"] = SWEEP_TRAFFIC_RATIO * p["bytes"] / max(p["launches"], 1)
-        out["traffic_note"] = ("dram__bytes_read+write per launch, scaled from an ncu capture of the forward "
-                               "sweep kernel on smooth_anomalies_56 (1.21x algorithmic)")
-    else:
-        out["traffic"] = None
     out["kernel"] = name
     out["launches"] = p["launches"]
     out["avg_launch_us"] = p["ms"] * 1e3 / max(p["launches"], 1)
@@ -361,60 +486,129 @@ def roofline_from_profile(prof, peaks):
     return out
 
 
-def cpu_baseline(w, iterations, steps=1):
+def roofline_from_profile(prof, peaks):
+    kernels = {k: v for k, v in prof.items() if k != "sweep" and v["launches"] > 0}
+    name = max(kernels, key=lambda k: kernels[k]["ms"])
+    out = roofline_entry(name, kernels[name], peaks)
+    if name == "solve_gemm":
+        out["traffic"] = SWEEP_TRAFFIC_RATIO * kernels[name]["bytes"] / max(kernels[name]["launches"], 1)
+        out["traffic_note"] = ("dram__bytes_read+write per launch, scaled from an ncu capture of the forward "
+                               "sweep kernel (1.21x algorithmic)")
+    else:
+        out["traffic"] = None
+    others = {n: roofline_entry(n, kernels[n], peaks) for n in ("stencil", "gmres_vector") if n in kernels}
+    return out, others
+
+
+def cpu_sample(w, its, kb, full_factor, steps, warmup):
+    """Bounded CPU sample of the workload with the FP64 oracle restatement
+    on every host thread: the global operator, one panel solve of the
+    bottom panel class for as many right-hand sides as threads, one matvec
+    of as many; the top panel's solve is scaled from it by its factor
+    nonzeros (the panel solve streams the factors), right-hand sides
+    linearly (they run one per thread).  With `full_factor` one bottom-class
+    panel is also factored (timed) and the top panel's factorization scaled
+    by its flops; otherwise the solves run on unit-diagonal fronts of the
+    panel's structure (same bytes and operations as real factors).  Returns
+    (modeled rates, per-step wall seconds, threads)."""
     import oracle
+    import psp_b200 as P
     d = w.disc
     O = oracle.Oracle(oracle.make_disc(d.omega, d.nx, d.ny, d.nz, d.wx, d.wy, d.wz,
                                        pml=(d.bx, d.by, d.bz), sigma=d.sigmax))
-    vals = []
-    for _ in range(steps):
-        t0 = time.time()
-        costs = oracle.sample_costs(O, w.velocity, w.k, reps=1)
-        m = oracle.modeled_rhs_per_s(O, costs, w.k, iterations)
-        m["sample_wall_s"] = time.time() - t0
-        vals.append(m)
-    best = max(vals, key=lambda m: m["rhs_per_s"])
-    return best, oracle.num_threads()
+    threads = oracle.num_threads()
+    geo = O.geometry()
+    np_ = geo.shape[0]
+    t0 = time.time()
+    O.form_operator(w.velocity)
+    t_op = time.time() - t0
+    # per-class factor nonzeros and flops (host analysis)
+    nnz, flops = {}, {}
+    for c in sorted(set(int(x) for x in geo[:, 3])):
+        info, _ = P.analyze_class(w.disc, 4, 12, c)
+        s, u = info[:, 1].astype(float), info[:, 2].astype(float)
+        nnz[c] = float(((s + u) * s - s * (s - 1) / 2).sum())
+        flops[c] = float((8 * (s ** 3 / 3 + s ** 2 * u) + 8 * s ** 3 / 6 + 8 * s ** 2 * u / 2 + 4 * s * u ** 2).sum())
+    p0 = 0
+    c0 = int(geo[p0, 3])
+    t_factor = oracle.time_factor_panel(O, w.velocity, p0) if full_factor else None
+    kS = max(1, min(threads, w.k))
+    walls, ps, mv = [], [], []
+    for i in range(warmup + steps):
+        t = time.time()
+        a = oracle.time_panel_solve(O, p0, kS)
+        b = oracle.time_multiply(O, kS)
+        if i >= warmup:
+            walls.append(time.time() - t)
+            ps.append(a)
+            mv.append(b)
+    oracle.release_panel(O, p0)
+    ps0 = min(ps) * w.k / kS
+    mvk = min(mv) * w.k / kS
+    sweep = sum((1 if p == np_ - 1 else 2) * ps0 * nnz[int(geo[p, 3])] / nnz[c0] for p in range(np_))
+    solve = (its + 1) * sweep + 2 * its * mvk
+    out = {"solve_only_rhs_per_s": w.k / solve, "modeled_solve_s": solve, "sweep_s": sweep,
+           "panel_solve_s": ps0, "matvec_s": mvk, "operator_s": t_op, "iterations": its}
+    if t_factor is not None:
+        setup = t_op + sum(t_factor * flops[int(geo[p, 3])] / flops[c0] for p in range(np_))
+        out.update({"factor_panel_s": t_factor, "modeled_setup_s": setup,
+                    "setup_plus_solve_rhs_per_s": w.k / (setup + solve)})
+    return out, walls, threads
 
 
-def workload(name):
-    from psp_b200 import workloads as W
-    return W.CONFIGS[name]()
+def workload_iterations(name, fallback):
+    return FP64_ITERATIONS.get(name) or fallback
+
+
+def model_check(name="plain_bump_50"):
+    """The sampled model next to a whole oracle Initialize + Solve of the
+    small FP64 reference case (seconds on the host cores)."""
+    import oracle
+    w = workload(name)
+    d = w.disc
+    m, _, _ = cpu_sample(w, workload_iterations(name, 20), w.k, True, 1, 0)
+    O = oracle.Oracle(oracle.make_disc(d.omega, d.nx, d.ny, d.nz, d.wx, d.wy, d.wz,
+                                       pml=(d.bx, d.by, d.bz), sigma=d.sigmax))
+    t0 = time.time()
+    O.initialize(w.velocity)
+    t1 = time.time()
+    _, st = O.solve(w.rhs, RESTART, REL_TOL)
+    t2 = time.time()
+    return {"workload": name, "iterations": st["iterations"],
+            "modeled_solve_only_rhs_per_s": m["solve_only_rhs_per_s"], "measured_solve_only_rhs_per_s": w.k / (t2 - t1),
+            "modeled_setup_plus_solve_rhs_per_s": m["setup_plus_solve_rhs_per_s"],
+            "measured_setup_plus_solve_rhs_per_s": w.k / (t2 - t0)}
 
 
 def main_reference(args):
-    """CPU arm: the FP64 oracle restatement of the reference on host cores."""
+    """CPU arm: the FP64 oracle restatement of the reference on the host
+    cores, a bounded sample of the same workload per step (cpu_sample),
+    reported in the same metric and config."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle
+    t_start = time.time()
     w = workload(args.config)
-    its = FP64_ITERATIONS.get(args.config) or 20
-    t0 = time.time()
-    d = w.disc
-    O = oracle.Oracle(oracle.make_disc(d.omega, d.nx, d.ny, d.nz, d.wx, d.wy, d.wz,
-                                       pml=(d.bx, d.by, d.bz), sigma=d.sigmax))
-    for _ in range(args.warmup):  # warm-up: operator formation + one matvec over the whole problem
-        O.form_operator(w.velocity)
-        O.multiply(w.rhs)
-    vals = []
-    for _ in range(args.steps):
-        m, cores = cpu_baseline(w, its, 1)
-        vals.append(m)
-    best = max(vals, key=lambda m: m["rhs_per_s"])
-    sample = ("oracle FP64 restatement on %d host threads; per step: global operator formation, one panel "
-              "factorization per panel class, one %d-RHS panel solve per class and one matvec on the full %s "
-              "workload, extrapolated to every panel and %d GMRES steps (2P-1 panel solves + 2 matvecs each)"
-              % (cores, w.k, args.config, its))
+    kb = BLOCK_WIDTH.get(args.config, w.k)
+    its = workload_iterations(args.config, 20)
+    m, walls, threads = cpu_sample(w, its, kb, True, args.steps, args.warmup)
+    value = m["solve_only_rhs_per_s"]
+    sample = ("oracle FP64 restatement on %d host threads; once: global operator and one factorization of the "
+              "bottom panel class (%.1f s, the top panel's scaled by its flops); per step: one solve of that "
+              "panel and one matvec for %d right-hand sides (threads run one each), scaled linearly to the "
+              "%d sources and, for the top panel, by its factor nonzeros; modeled Solve = (%d GMRES steps + 1) "
+              "sweeps of 2P-1 panel solves + 2 matvecs per step" %
+              (threads, m.get("factor_panel_s", 0.0), min(threads, w.k), w.k, its))
+    check = model_check()
     line = {
-        "metric": METRIC, "value": best["rhs_per_s"], "unit": UNIT, "impl": "reference", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * w.k / best["rhs_per_s"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": args.config, "grid": [w.disc.nx, w.disc.ny, w.disc.nz], "k": w.k},
-        "cpu_baseline": {"value": best["rhs_per_s"], "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": best["rhs_per_s"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "solve_only_rhs_per_s": best["solve_only_rhs_per_s"], "wall_s": time.time() - t0,
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic", "config": config_dict(args.config, w, kb),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "model": m, "model_check": check, "wall_s": time.time() - t_start,
     }
     print(json.dumps(line), flush=True)
 
@@ -433,100 +627,83 @@ def main():
     torch.cuda.set_device(local)
     w = workload(args.config)
     N = w.disc.nx * w.disc.ny * w.disc.nz
-    k = w.k
     vel_d = torch.from_numpy(w.velocity.reshape(-1)).to("cuda")
-    rhs_d = torch.from_numpy(w.rhs.reshape(-1)).to("cuda")
-    X = torch.empty_like(rhs_d)
     H = P.DistHelmholtz(w.disc, device=local)
     stream = torch.cuda.ExternalStream(H.stream_ptr(), device=torch.device("cuda", local))
     peaks = load_peaks()
 
+    # mixed precision: Initialize timed apart, then block Solve steps
+    setup_ms = time_initialize(H, vel_d, P.MIXED, 2, stream)
+    kb = H.solve_block_width(w.k, RESTART)
     clocks = ClockSampler(local)
-    mixed = run_arm(H, w, vel_d, rhs_d, X, P.MIXED, args.steps, args.warmup, ws, stream, clocks)
-    X_mixed = X.clone()
+    mixed = solve_steps(H, w, kb, args.steps, args.warmup, ws, stream, clocks)
     st_m = mixed["stats"][-1]
-    value = ws * k * args.steps / (mixed["total_ms"] * 1e-3)
-    solve_only = ws * k * args.steps / (mixed["solve_ms"] * 1e-3)
-
-    fp64 = None
-    if not args.no_fp64:
-        f = run_arm(H, w, vel_d, rhs_d, X, P.FP64, args.steps, max(1, args.warmup - 2), ws, stream)
-        st_f = f["stats"][-1]
-        err = float(torch.linalg.norm(X_mixed - X) / torch.linalg.norm(X))
-        fp64 = {"value": ws * k * args.steps / (f["total_ms"] * 1e-3),
-                "solve_only_rhs_per_s": ws * k * args.steps / (f["solve_ms"] * 1e-3),
-                "ms_per_step": f["total_ms"] / args.steps, "setup_ms_per_step": f["setup_ms"] / args.steps,
-                "iterations": st_f["iterations"], "final_rel_resid": st_f["final_max_rel_resid"],
-                "mixed_rel_diff_vs_fp64": err}
+    value = ws * mixed["rhs"] / (mixed["total_ms"] * 1e-3)
+    setup_s = max_over_ranks(statistics.mean(setup_ms), ws) * 1e-3
+    block_s = mixed["total_ms"] * 1e-3 / args.steps
+    nb = math.ceil(w.k / kb)
+    setup_plus_solve = w.k / (setup_s + nb * block_s)
+    # the first block's mixed wavefields, for the FP64 comparison
+    X0 = w.rhs_torch("cuda", cols=block_cols(w, kb, 0))
+    H.Solve(X0, RESTART, REL_TOL)
+    mixed_block0 = X0.cpu().numpy().reshape(N, -1)
+    del X0, mixed["X"]
+    prof = profile_block(H, w, kb, stream)
+    roof, other_roofs = roofline_from_profile(prof, peaks)
+    launches_per_step = sum(v["launches"] for n, v in prof.items() if n != "sweep")
+    mem_mixed = H.memory_info()
 
     e2e = None
     if not args.no_e2e:
         vel_h = np.ascontiguousarray(w.velocity.reshape(-1))
-        rhs_h = np.ascontiguousarray(w.rhs.reshape(-1))
-        B_h = np.empty_like(rhs_h)
-        # one untimed call: the handle's pinned staging and device scratch
-        H.Initialize(vel_h, precision=P.MIXED)
-        B_h[:] = rhs_h
-        H.Solve(B_h, RESTART, REL_TOL)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        barrier(ws)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(args.steps):
-            H.Initialize(vel_h, precision=P.MIXED)
-            B_h[:] = rhs_h
-            H.Solve(B_h, RESTART, REL_TOL)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws)
-        e2e = {"value": ws * k * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
-               "h2d_bytes_per_step": int(N * 8 + N * k * 16), "d2h_bytes_per_step": int(N * k * 16)}
+        e2e = e2e_arm(H, w, vel_h, kb, max(1, min(args.steps, nb)), ws, stream)
+
+    H.Finalize()
+    torch.cuda.empty_cache()
+    fp64 = None
+    if not args.no_fp64:
+        fp64 = fp64_sample(H, w, vel_d, stream, mixed_block0)
+        H.Finalize()
+        torch.cuda.empty_cache()
 
     batch = None
     if not args.no_batch:
-        H.Finalize()
         batch = batch_arm(args, ws, rank, local)
 
     grad = None
     if not args.no_grad:
-        H.Finalize()
         grad = gradient_arm(args, ws, local)
-
-    prof = profile_step(H, vel_d, rhs_d, X, P.MIXED, stream)
-    roof = roofline_from_profile(prof, peaks)
-    launches_per_step = sum(v["launches"] for n, v in prof.items() if n != "sweep")
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        its = fp64["iterations"] if fp64 else st_m["iterations"]
-        m, cores = cpu_baseline(w, its)
-        cpu = {"value": m["rhs_per_s"], "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": ("oracle FP64 restatement on %d host threads: global operator, one panel factorization "
-                          "and one %d-RHS panel solve per panel class and one matvec of the full workload, "
-                          "timed once (%.1f s) and extrapolated to every panel and %d GMRES steps" %
-                          (cores, k, m["sample_wall_s"], its)),
-               "solve_only_rhs_per_s": m["solve_only_rhs_per_s"], "modeled_setup_s": m["setup_seconds"],
-               "modeled_solve_s": m["solve_seconds"]}
+        its = workload_iterations(args.config, fp64["iterations"] if fp64 else st_m["iterations"])
+        m, walls, threads = cpu_sample(w, its, kb, False, 2, 0)
+        cpu = {"value": m["solve_only_rhs_per_s"], "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": ("oracle FP64 restatement on %d host threads: one bottom-class panel solve and one "
+                          "matvec for %d right-hand sides on the full workload (%.1f s of CPU work), scaled to "
+                          "the %d sources, every panel (top panel by its factor nonzeros) and %d GMRES steps"
+                          % (threads, min(threads, w.k), sum(walls), w.k, its)),
+               "model": m}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mixed["total_ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 fronts/sweeps + c128 GMRES",
-            "data": "synthetic",
-            "config": {"workload": args.config, "grid": [w.disc.nx, w.disc.ny, w.disc.nz], "interior": w.interior,
-                       "pml": w.pml, "k": k, "gmres_restart": RESTART, "rel_tol": REL_TOL,
-                       "step": "Initialize + Solve", "l2": "inputs larger than L2 (factors > 10 GB)",
-                       "parallelism": "independent problem per GPU"},
-            "solve_only_rhs_per_s": solve_only,
-            "setup_ms_per_step": mixed["setup_ms"] / args.steps,
+            "data": "synthetic", "config": config_dict(args.config, w, kb),
+            "setup_ms": 1e3 * setup_s, "setup_plus_solve_rhs_per_s": setup_plus_solve,
             "iterations": st_m["iterations"], "final_rel_resid": st_m["final_max_rel_resid"],
+            "converged": all(s["converged"] for s in mixed["stats"]),
+            "memory": mem_mixed,
             "fp64": fp64,
             "mixed_over_fp64": (value / fp64["value"]) if fp64 else None,
+            "mixed_over_fp64_setup_plus_solve": (setup_plus_solve / fp64["setup_plus_solve_rhs_per_s"])
+            if fp64 else None,
             "e2e": e2e,
             "gradients_per_s": grad,
             "batch": batch,
             "roofline": roof,
+            "rooflines_other": other_roofs,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": int(launches_per_step * args.steps),

@@ -188,6 +188,25 @@ int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info);
 /* Seconds spent in the last Initialize and bytes of stored panel factors. */
 int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* factor_bytes);
 
+/* Factor storage after Initialize (no counterpart in the reference, whose
+ * panels are always resident across its MPI ranks): the number of panels
+ * whose factors stay in device memory out of num_panels, the panel
+ * factorizations sweeps have rerun since Initialize for the others (each
+ * recomputed panel is factored again into a per-class slot whenever a sweep
+ * reaches it), and the bytes of the handle's scratch (factorization
+ * transients, then the GMRES workspace).  Residency is decided at the first
+ * Initialize from free device memory; PSP_B200_RESIDENT_PANELS caps it and
+ * PSP_B200_SOLVE_RESERVE_RHS sets the right-hand sides whose GMRES
+ * workspace is kept free (default 16). */
+int psp_cu_memory_info(const psp_cu_handle* h, int* resident_panels, int* num_panels, long long* refactorizations,
+                       long long* scratch_bytes);
+
+/* Right-hand sides per GMRES block that Solve of k right-hand sides with
+ * restart m would use now: k when the workspace of all of them fits beside
+ * the factors, else the width of the equal blocks it solves one after
+ * another (no counterpart in the reference, which holds all k at once). */
+int psp_cu_solve_block_width(psp_cu_handle* h, int k, int m, int* width);
+
 /* The CUDA stream (cudaStream_t) all work of the handle is issued on. */
 int psp_cu_get_stream(const psp_cu_handle* h, void** stream);
 

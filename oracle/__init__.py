@@ -231,6 +231,44 @@ def modeled_rhs_per_s(orc, costs, k, iterations, restarts=1):
                 rhs_per_s=k / (setup + solve), solve_only_rhs_per_s=k / solve)
 
 
+def time_factor_panel(orc, velocity, p):
+    """Seconds of one panel factorization (panel p's fronts are kept)."""
+    L = lib()
+    L.oracle_time_factor_panel.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)]
+    v = np.ascontiguousarray(velocity, dtype=np.float64)
+    t = ctypes.c_double()
+    if L.oracle_time_factor_panel(orc._h, _ptr(v), p, ctypes.byref(t)):
+        raise RuntimeError(L.oracle_last_error().decode())
+    return t.value
+
+
+def time_panel_solve(orc, p, k):
+    """Seconds of one panel solve of k right-hand sides (unit-diagonal zero
+    fronts of the panel's structure stand in when it holds no factors)."""
+    L = lib()
+    L.oracle_time_panel_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    t = ctypes.c_double()
+    if L.oracle_time_panel_solve(orc._h, p, k, ctypes.byref(t)):
+        raise RuntimeError(L.oracle_last_error().decode())
+    return t.value
+
+
+def release_panel(orc, p):
+    lib().oracle_release_panel.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib().oracle_release_panel(orc._h, p)
+
+
+def time_multiply(orc, k):
+    """Seconds of one global matvec of k right-hand sides."""
+    L = lib()
+    L.oracle_time_multiply.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    t = ctypes.c_double()
+    if L.oracle_time_multiply(orc._h, k, ctypes.byref(t)):
+        raise RuntimeError(L.oracle_last_error().decode())
+    return t.value
+
+
 def num_threads():
     lib().oracle_num_threads.restype = ctypes.c_int
     return lib().oracle_num_threads()

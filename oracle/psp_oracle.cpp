@@ -1138,6 +1138,89 @@ int oracle_sample(void* h, const double* velocity, int k, int reps, double* out)
     }
 }
 
+// Bounded timing pieces for workloads too large for a whole CPU solve.
+// Each returns the wall seconds of one piece of Initialize or Solve on the
+// handle's own problem (threads as for the full solve).
+//
+// Factors panel p (FactorPanel, the cliq::LDL stand-in) and keeps its fronts.
+int oracle_time_factor_panel(void* h, const double* velocity, int p, double* seconds) {
+    Solver& S = *(Solver*)h;
+    try {
+        if (p < 0 || p >= S.numPanels) throw std::runtime_error("panel index out of range");
+        if ((int)S.fronts.size() != S.numPanels) S.fronts.assign(S.numPanels, std::vector<Front>());
+        const double t = omp_get_wtime();
+        FactorPanel(S, p, velocity);
+        *seconds = omp_get_wtime() - t;
+        return 0;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+// SolvePanel of panel p (solve.hpp:736-882) on k seeded right-hand sides.
+// When panel p holds no factors, fronts of its structure are allocated with
+// a unit diagonal and zeros elsewhere: the solve then streams exactly the
+// bytes and does exactly the operations it does on real factors (operand
+// values do not change the cost of FP64 arithmetic away from denormals),
+// without a factorization first.
+int oracle_time_panel_solve(void* h, int p, int k, double* seconds) {
+    Solver& S = *(Solver*)h;
+    try {
+        if (p < 0 || p >= S.numPanels) throw std::runtime_error("panel index out of range");
+        if ((int)S.fronts.size() != S.numPanels) S.fronts.assign(S.numPanels, std::vector<Front>());
+        std::vector<Front>& fr = S.fronts[p];
+        if (fr.empty()) {
+            const PanelTree& T = S.trees[PanelClass(S, p)];
+            fr.assign(T.nodes.size(), Front());
+            for (size_t t = 0; t < T.nodes.size(); ++t) {
+                Front& f = fr[t];
+                f.s = T.nodes[t].size;
+                f.u = (int)T.nodes[t].lower.size();
+                f.L.assign((size_t)(f.s + f.u) * f.s, C(0));
+                for (int j = 0; j < f.s; ++j) f.L[(size_t)j * (f.s + f.u) + j] = C(1);
+            }
+        }
+        std::vector<C> B((size_t)S.N * k);
+        uint64_t seed = 2024;
+        for (auto& v : B) {
+            seed = seed * 6364136223846793005ULL + 1442695040888963407ULL;
+            v = C(((seed >> 11) & 0xFFFFF) / double(0xFFFFF) - 0.5, ((seed >> 33) & 0xFFFFF) / double(0xFFFFF) - 0.5);
+        }
+        const double t = omp_get_wtime();
+        SolvePanel(S, B.data(), k, p);
+        *seconds = omp_get_wtime() - t;
+        return 0;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+// Frees the fronts of panel p.
+int oracle_release_panel(void* h, int p) {
+    Solver& S = *(Solver*)h;
+    if (p >= 0 && p < (int)S.fronts.size()) std::vector<Front>().swap(S.fronts[p]);
+    return 0;
+}
+
+// Multiply (solve.hpp:613-679) of k seeded right-hand sides; the global
+// operator must have been formed (oracle_form_operator).
+int oracle_time_multiply(void* h, int k, double* seconds) {
+    Solver& S = *(Solver*)h;
+    try {
+        if (S.vals.empty()) throw std::runtime_error("the global operator has not been formed");
+        std::vector<C> B((size_t)S.N * k, C(0.25, -0.5));
+        const double t = omp_get_wtime();
+        Multiply(S, B.data(), k);
+        *seconds = omp_get_wtime() - t;
+        return 0;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 int oracle_num_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -75,6 +75,7 @@ C_ABI_SYMBOLS = [
     "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device", "psp_cu_initialize_batch", "psp_cu_solve_batch",
     "psp_cu_grid_load", "psp_cu_grid_interpolate", "psp_cu_grid_write_plane", "psp_cu_grid_write_volume",
     "psp_cu_set_view_iterates", "psp_cu_set_ritz_values", "psp_cu_get_ritz_values", "psp_cu_hessenberg_eigenvalues",
+    "psp_cu_memory_info", "psp_cu_solve_block_width",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -132,6 +133,9 @@ def lib():
         L.psp_cu_set_ritz_values.argtypes = [vp, ci]
         L.psp_cu_get_ritz_values.argtypes = [vp, ip, ip, dp]
         L.psp_cu_hessenberg_eigenvalues.argtypes = [ci, dp, ci, dp]
+        L.psp_cu_solve_block_width.argtypes = [vp, ci, ci, ip]
+        L.psp_cu_memory_info.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
     return _lib
 
@@ -453,6 +457,21 @@ class DistHelmholtz:
         b = ctypes.c_longlong()
         _check(lib().psp_cu_setup_info(self._h, ctypes.byref(s), ctypes.byref(b)))
         return s.value, b.value
+
+    def memory_info(self):
+        """Factor storage: dict(resident_panels, num_panels,
+        refactorizations, scratch_bytes) (psp_cu_memory_info)."""
+        r, n = ctypes.c_int(), ctypes.c_int()
+        f, b = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(lib().psp_cu_memory_info(self._h, ctypes.byref(r), ctypes.byref(n), ctypes.byref(f), ctypes.byref(b)))
+        return dict(resident_panels=r.value, num_panels=n.value, refactorizations=f.value, scratch_bytes=b.value)
+
+    def solve_block_width(self, k, m=20):
+        """Right-hand sides per GMRES block that Solve of k right-hand sides
+        would use now (psp_cu_solve_block_width)."""
+        wd = ctypes.c_int()
+        _check(lib().psp_cu_solve_block_width(self._h, int(k), int(m), ctypes.byref(wd)))
+        return wd.value
 
     def _grid_op(self, fn, B, *extra):
         X = np.ascontiguousarray(B, dtype=np.complex128).copy()

@@ -352,6 +352,25 @@ int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* 
     return PSP_CU_OK;
 }
 
+int psp_cu_memory_info(const psp_cu_handle* h, int* resident_panels, int* num_panels, long long* refactorizations,
+                       long long* scratch_bytes) {
+    if (int e = CheckHandle(h)) return e;
+    if (resident_panels) *resident_panels = h->solver->ResidentPanels();
+    if (num_panels) *num_panels = h->solver->analysis().geom.numPanels;
+    if (refactorizations) *refactorizations = (long long)h->solver->Refactorizations();
+    if (scratch_bytes) *scratch_bytes = (long long)h->solver->ScratchBytes();
+    return PSP_CU_OK;
+}
+
+int psp_cu_solve_block_width(psp_cu_handle* h, int k, int m, int* width) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!width) throw PspError(PSP_CU_LOGIC_ERROR, "null output");
+        CUDA_CHECK(cudaSetDevice(h->solver->device()));
+        *width = h->solver->SolveBlockWidth(k, m);
+    });
+}
+
 int psp_cu_grid_load(const char* filename, int nx, int ny, int nz, int num_scalars, int is_complex, int order,
                      double* d_out) {
     return Guard([&] {

@@ -9,6 +9,8 @@
 // breaks the capture), and services that reserve all device memory at
 // start-up and treat any later allocation as an error.
 //
+// The caller's current device is current again when the call returns.
+//
 // Limits and sharing: the array holds kNoAllocMaxEntries complex doubles
 // (16 MiB); every GPU that loads this library holds it until the process
 // exits.  All calls on a device share the one array and it keeps the last
@@ -52,7 +54,21 @@ namespace psp_b200 {
 void SetLastError(const std::string& msg);  // capi.cu: text returned by psp_cu_last_error
 }
 
+namespace {
+// Makes the caller's current device current again when the call returns.
+struct RestoreDevice {
+    int device = -1;
+    RestoreDevice() {
+        if (cudaGetDevice(&device) != cudaSuccess) device = -1;
+    }
+    ~RestoreDevice() {
+        if (device >= 0) cudaSetDevice(device);
+    }
+};
+}  // namespace
+
 extern "C" int psp_cu_multiply_device_noalloc(psp_cu_handle* h, double* d_B, int k) {
+    RestoreDevice restore;
     try {
         if (!h || !h->solver || !d_B) throw psp_b200::PspError(PSP_CU_LOGIC_ERROR, "null argument");
         psp_b200::Helmholtz& s = *h->solver;
@@ -64,9 +80,7 @@ extern "C" int psp_cu_multiply_device_noalloc(psp_cu_handle* h, double* d_B, int
                                      "grid too large for the allocation-free multiply: nx*ny*nz*k = " +
                                          std::to_string(entries) + " exceeds " +
                                          std::to_string(kNoAllocMaxEntries));
-        int device = 0;
-        CUDA_CHECK(cudaGetDevice(&device));
-        if (device != s.device_) CUDA_CHECK(cudaSetDevice(s.device_));
+        if (restore.device != s.device_) CUDA_CHECK(cudaSetDevice(s.device_));
         if (s.device_ >= kMaxDevices) throw psp_b200::PspError(PSP_CU_LOGIC_ERROR, "device index too large");
         psp_b200::z64* scratch = ScratchOnDevice(s.device_);
         psp_b200::z64* B = reinterpret_cast<psp_b200::z64*>(d_B);

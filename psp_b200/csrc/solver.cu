@@ -166,11 +166,34 @@ public:
         for (auto& g : graphs_) cudaGraphExecDestroy(g.exec);
     }
     void Factor();
+    // Makes panel p's factors available: a recomputed panel is factored
+    // into its class's slot unless the slot holds it already.
+    void EnsurePanel(int p);
     void SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc);
     // One sweep (Precondition); replayed from a captured CUDA graph when
     // `useGraph` and profiling is off.
     void Sweep(z64* B, int ldk, int k, bool useGraph);
-    int64_t Bytes() const { return (int64_t)(G_.bytes + D_.bytes); }
+    int64_t Bytes() const {
+        int64_t b = (int64_t)(G_.bytes + D_.bytes);
+        for (int c = 0; c < 3; ++c) b += (int64_t)(slotG_[c].bytes + slotD_[c].bytes);
+        return b;
+    }
+    int ResidentPanels() const {
+        int n = 0;
+        for (char r : resident_) n += r;
+        return n;
+    }
+    int64_t Refactorizations() const { return refactors_; }
+    // Device bytes of the solve plan per right-hand side (work vectors).
+    double PlanBytesPerRhs() const;
+    bool HasPlan(int k) const {
+        for (const auto& pl : plans_)
+            if (pl->k == k) return true;
+        return false;
+    }
+    // Frees the solve plans (and the sweep graphs that use them) of every
+    // block width but k.
+    void DropPlansExcept(int k);
     // Device status word: bit 1 zero/non-finite pivot, bit 2 a tensor-core
     // pipeline wait timed out.  Synchronizes the stream.
     int ReadStatus() {
@@ -198,25 +221,49 @@ private:
     std::vector<SweepGraph> graphs_;
     void SweepEager(z64* B, int ldk, int k);
     // The factorization of one group of panels as recorded launches: its
-    // transient buffers, uploaded task lists and steps.  When every panel
-    // fits in one group the program is kept, and a later Initialize of the
-    // same handle (same structure, new velocity) only replays it.
+    // uploaded task lists and steps, with the transient buffers at a fixed
+    // place (the handle's scratch for the resident panels, the recompute
+    // arena for a recomputed panel).  Programs are kept, so a later
+    // Initialize of the same handle (same structure, new velocity) only
+    // replays them while the scratch has not moved.
     struct FactorProgram {
-        DeviceBuffer arena;
+        unsigned char* arena = nullptr;
+        size_t arenaBytes = 0;
         TaskArena tasks;
         std::vector<Step> steps;
         size_t frontsOff = 0;
     };
     std::vector<std::unique_ptr<FactorProgram>> program_;
-    void FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& all, bool keep);
-    void RunProgram(FactorProgram& pg);
+    // Transient bytes of the factorization of `panels` at its busiest depth.
+    int64_t TransientBytes(const std::vector<int>& panels) const;
+    std::unique_ptr<FactorProgram> FactorGroup(const std::vector<int>& panels, unsigned char* arena,
+                                               size_t arenaBytes);
+    void RunProgram(FactorProgram& pg, bool sync);
     void CheckPivots();
+    // Storage of the factors: which panels stay resident, where each
+    // front's G and D live, and the slots of the recomputed panels.
+    void BuildLayout();
 
     Helmholtz& h_;
     const Analysis& an_;
     int nn_ = 0;  // nodes per panel tree
+    bool layout_ = false;
     DeviceBuffer G_, D_;
-    std::vector<int64_t> gOff_, dOff_;
+    std::vector<int64_t> gOff_, dOff_;    // per (panel, node): offset in its panel's storage
+    std::vector<cpx<R>*> gPtr_, dPtr_;     // per (panel, node): where G and D live
+    std::vector<char> resident_;           // per panel
+    std::vector<FactorFront<R>> fronts_;   // per (panel, node), transient pointers unset
+    // Recomputed panels: one slot per class for G and D, the arena of their
+    // factorization transients, their programs and what each slot holds.
+    DeviceBuffer slotG_[3], slotD_[3], rarena_;
+    std::vector<std::unique_ptr<FactorProgram>> recompute_;  // per panel (null when resident)
+    int slotHolds_[3] = {-1, -1, -1};
+    int64_t refactors_ = 0;
+    bool AllResident() const {
+        for (char r : resident_)
+            if (!r) return false;
+        return true;
+    }
     std::vector<std::vector<int>> depthNodes_;
     DeviceBuffer status_;
     // One way to run the solve GEMM of one depth and direction: the kernel
@@ -260,7 +307,8 @@ private:
     // class (scratch right-hand sides; without room for them the default
     // tiling stays) and keeps the fastest per depth and direction.  Events
     // bracket each solve-GEMM launch while tune_ is set.
-    void Autotune(SolvePlan& P);
+    // Returns false when it measured nothing (no room for its scratch).
+    bool Autotune(SolvePlan& P);
     struct TuneEvents {
         std::vector<cudaEvent_t> ev;
         int used = 0;
@@ -277,13 +325,40 @@ private:
 };
 
 template <typename R>
-void FactorStore<R>::Factor() {
-    if (!program_.empty()) {  // same structure as the last factorization: replay it
-        CUDA_CHECK(cudaMemsetAsync(status_.p, 0, sizeof(int), h_.stream_));
-        for (auto& pg : program_) RunProgram(*pg);
-        CheckPivots();
-        return;
+int64_t FactorStore<R>::TransientBytes(const std::vector<int>& panels) const {
+    const PanelGeometry& g = an_.geom;
+    const size_t nd = depthNodes_.size();
+    std::vector<int64_t> L(nd, 0), U(nd, 0), T(nd, 0);
+    for (size_t d = 0; d < nd; ++d)
+        for (int p : panels) {
+            const ClassStructure& cs = an_.cls[g.Class(p)];
+            for (int t : depthNodes_[d]) {
+                const int64_t s = cs.size[t], u = cs.usize[t];
+                L[d] += (s + u) * s;
+                U[d] += u * u;
+                T[d] += (s / 2 + 1) * (s / 2 + 1) * 2;
+            }
+        }
+    int64_t ua = 0, ub = 0, lm = 0, tm = 0;
+    for (size_t d = 0; d < nd; ++d) {
+        (d % 2 ? ub : ua) = std::max(d % 2 ? ub : ua, U[d]);
+        lm = std::max(lm, L[d]);
+        tm = std::max(tm, T[d]);
     }
+    return (ua + ub + lm + tm) * (int64_t)sizeof(cpx<R>);
+}
+
+// Environment integer, or `dflt` when unset or not a number.
+static long long EnvInt(const char* name, long long dflt) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    char* end = nullptr;
+    const long long x = std::strtoll(v, &end, 10);
+    return (end && *end == 0) ? x : dflt;
+}
+
+template <typename R>
+void FactorStore<R>::BuildLayout() {
     const PanelGeometry& g = an_.geom;
     const XYTree& tree = an_.tree;
     nn_ = (int)tree.nodes.size();
@@ -291,33 +366,123 @@ void FactorStore<R>::Factor() {
     depthNodes_.assign(tree.maxDepth + 1, {});
     for (int t = 0; t < nn_; ++t) depthNodes_[tree.nodes[t].depth].push_back(t);
 
+    // per-panel storage: G then D of every front, offsets inside the panel
     gOff_.assign((size_t)np * nn_, 0);
     dOff_.assign((size_t)np * nn_, 0);
-    int64_t gTot = 0, dTot = 0;
+    std::vector<int64_t> gPanel(np, 0), dPanel(np, 0);
     for (int p = 0; p < np; ++p) {
         const ClassStructure& cs = an_.cls[g.Class(p)];
         for (int t = 0; t < nn_; ++t) {
-            gOff_[(size_t)p * nn_ + t] = gTot;
-            dOff_[(size_t)p * nn_ + t] = dTot;
-            gTot += (int64_t)GLeadingDim(cs.size[t], cs.usize[t]) * cs.size[t];
-            dTot += cs.size[t];
+            gOff_[(size_t)p * nn_ + t] = gPanel[p];
+            dOff_[(size_t)p * nn_ + t] = dPanel[p];
+            gPanel[p] += (int64_t)GLeadingDim(cs.size[t], cs.usize[t]) * cs.size[t];
+            dPanel[p] += cs.size[t];
         }
     }
-    G_.Allocate(gTot * sizeof(cpx<R>));
-    D_.Allocate(dTot * sizeof(cpx<R>));
+    auto panelBytes = [&](int p) { return (gPanel[p] + dPanel[p]) * (int64_t)sizeof(cpx<R>); };
+
+    // Which panels stay resident.  The factors of all panels are kept when
+    // they fit beside a reserve for the solve (the GMRES workspace of
+    // PSP_B200_SOLVE_RESERVE_RHS right-hand sides at restart 20, default
+    // 16) and a margin; otherwise the top panel (the costliest to factor)
+    // and the lowest others are kept and the rest are recomputed into one
+    // slot per class whenever a sweep reaches them (the highest panels: the
+    // last one the forward sweep recomputes is the first the backward sweep
+    // needs, so the slot still holds it).  PSP_B200_RESIDENT_PANELS caps the
+    // resident count (0: every panel recomputed).
+    size_t freeB = 0, totalB = 0;
+    CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
+    const double avail = (double)freeB + (double)h_.ScratchBytes();
+    const double reserveRhs = (double)EnvInt("PSP_B200_SOLVE_RESERVE_RHS", 16);
+    const double reserve = reserveRhs * (double)h_.NumUnknowns() * sizeof(z64) * 25 + 1.0e9 + 0.02 * totalB;
+    const long long cap = EnvInt("PSP_B200_RESIDENT_PANELS", -1);
+    std::vector<int> order;  // residency priority
+    order.push_back(np - 1);
+    for (int p = 0; p < np - 1; ++p) order.push_back(p);
+    resident_.assign(np, 1);
+    double all = 0;
+    for (int p = 0; p < np; ++p) all += (double)panelBytes(p);
+    if (cap >= 0 || all > avail - reserve) {
+        // room for the slots and the recompute arena of every class that
+        // may lose a panel (all classes but the top panel's, unless capped
+        // to nothing), then panels in priority order while they fit
+        double extra = 0;
+        for (int c = 0; c < 3; ++c) {
+            if (!an_.classUsed[c]) continue;
+            std::vector<int> one;
+            int64_t pb = 0;
+            for (int p = 0; p < np; ++p)
+                if (g.Class(p) == c && (p != np - 1 || cap == 0)) {
+                    if (one.empty()) one.push_back(p);
+                    pb = std::max(pb, panelBytes(p));
+                }
+            if (one.empty()) continue;
+            extra += (double)pb + (double)TransientBytes(one);
+        }
+        double used = 0;
+        int count = 0;
+        resident_.assign(np, 0);
+        for (int p : order) {
+            if (cap >= 0 && count >= cap) break;
+            if (used + (double)panelBytes(p) > avail - reserve - extra) break;
+            resident_[p] = 1;
+            used += (double)panelBytes(p);
+            ++count;
+        }
+    }
+    int64_t gTot = 0, dTot = 0;
+    for (int p = 0; p < np; ++p)
+        if (resident_[p]) { gTot += gPanel[p]; dTot += dPanel[p]; }
+    G_.Allocate(std::max<int64_t>(gTot, 1) * sizeof(cpx<R>));
+    D_.Allocate(std::max<int64_t>(dTot, 1) * sizeof(cpx<R>));
     CUDA_CHECK(cudaMemsetAsync(G_.p, 0, G_.bytes, h_.stream_));
+    std::vector<int64_t> gBase(np, 0), dBase(np, 0);
+    {
+        int64_t gb = 0, db = 0;
+        for (int p = 0; p < np; ++p)
+            if (resident_[p]) { gBase[p] = gb; dBase[p] = db; gb += gPanel[p]; db += dPanel[p]; }
+    }
+    int64_t slotBytesG[3] = {0, 0, 0}, slotBytesD[3] = {0, 0, 0};
+    std::vector<int> recomputed[3];
+    for (int p = 0; p < np; ++p)
+        if (!resident_[p]) {
+            const int c = g.Class(p);
+            slotBytesG[c] = std::max(slotBytesG[c], gPanel[p]);
+            slotBytesD[c] = std::max(slotBytesD[c], dPanel[p]);
+            recomputed[c].push_back(p);
+        }
+    int64_t rarenaBytes = 0;
+    for (int c = 0; c < 3; ++c) {
+        if (recomputed[c].empty()) continue;
+        slotG_[c].Allocate(slotBytesG[c] * sizeof(cpx<R>));
+        slotD_[c].Allocate(slotBytesD[c] * sizeof(cpx<R>));
+        CUDA_CHECK(cudaMemsetAsync(slotG_[c].p, 0, slotG_[c].bytes, h_.stream_));
+        rarenaBytes = std::max(rarenaBytes, TransientBytes({recomputed[c][0]}));
+    }
+    if (rarenaBytes) rarena_.Allocate(rarenaBytes);
+    gPtr_.assign((size_t)np * nn_, nullptr);
+    dPtr_.assign((size_t)np * nn_, nullptr);
+    for (int p = 0; p < np; ++p) {
+        const int c = g.Class(p);
+        cpx<R>* gp = resident_[p] ? G_.as<cpx<R>>() + gBase[p] : slotG_[c].template as<cpx<R>>();
+        cpx<R>* dp = resident_[p] ? D_.as<cpx<R>>() + dBase[p] : slotD_[c].template as<cpx<R>>();
+        for (int t = 0; t < nn_; ++t) {
+            gPtr_[(size_t)p * nn_ + t] = gp + gOff_[(size_t)p * nn_ + t];
+            dPtr_[(size_t)p * nn_ + t] = dp + dOff_[(size_t)p * nn_ + t];
+        }
+    }
     status_.Allocate(sizeof(int));
     CUDA_CHECK(cudaMemsetAsync(status_.p, 0, sizeof(int), h_.stream_));
 
-    std::vector<FactorFront<R>> all((size_t)np * nn_);
+    fronts_.assign((size_t)np * nn_, FactorFront<R>());
     for (int p = 0; p < np; ++p) {
         const int c = g.Class(p);
         const ClassStructure& cs = an_.cls[c];
         for (int t = 0; t < nn_; ++t) {
-            FactorFront<R>& f = all[(size_t)p * nn_ + t];
+            FactorFront<R>& f = fronts_[(size_t)p * nn_ + t];
             std::memset(&f, 0, sizeof(f));
-            f.G = G_.as<cpx<R>>() + gOff_[(size_t)p * nn_ + t];
-            f.D = D_.as<cpx<R>>() + dOff_[(size_t)p * nn_ + t];
+            f.G = gPtr_[(size_t)p * nn_ + t];
+            f.D = dPtr_[(size_t)p * nn_ + t];
             f.rel = h_.dRel_[c].as<int>() + cs.lowerOff[t];
             f.s = cs.size[t];
             f.u = cs.usize[t];
@@ -329,35 +494,64 @@ void FactorStore<R>::Factor() {
             f.s3aOff = h_.s3aOff_[p];
         }
     }
-    // Transient bytes a group of panels needs at its busiest depth.
-    auto transient = [&](int p0, int p1) {
-        std::vector<int64_t> L(depthNodes_.size(), 0), U(depthNodes_.size(), 0), T(depthNodes_.size(), 0);
-        for (size_t d = 0; d < depthNodes_.size(); ++d)
-            for (int p = p0; p < p1; ++p) {
-                const ClassStructure& cs = an_.cls[g.Class(p)];
-                for (int t : depthNodes_[d]) {
-                    const int64_t s = cs.size[t], u = cs.usize[t];
-                    L[d] += (s + u) * s;
-                    U[d] += u * u;
-                    T[d] += (s / 2 + 1) * (s / 2 + 1) * 2;
-                }
-            }
-        int64_t ua = 0, ub = 0, lm = 0, tm = 0;
-        for (size_t d = 0; d < depthNodes_.size(); ++d) {
-            (d % 2 ? ub : ua) = std::max(d % 2 ? ub : ua, U[d]);
-            lm = std::max(lm, L[d]);
-            tm = std::max(tm, T[d]);
-        }
-        return (ua + ub + lm + tm) * (int64_t)sizeof(cpx<R>);
-    };
-    size_t freeB = 0, totalB = 0;
-    CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
-    const int64_t budget = (int64_t)(freeB * 0.8);
-    int groupSize = np;
-    while (groupSize > 1 && transient(0, groupSize) > budget) groupSize = (groupSize + 1) / 2;
-    for (int p0 = 0; p0 < np; p0 += groupSize)
-        FactorGroup(p0, std::min(np, p0 + groupSize), all, groupSize == np);
+    // recomputed panels: one program each, transients in the recompute arena
+    recompute_.clear();
+    recompute_.resize(np);
+    for (int p = 0; p < np; ++p)
+        if (!resident_[p])
+            recompute_[p] = FactorGroup({p}, rarena_.template as<unsigned char>(), rarena_.bytes);
+    layout_ = true;
+}
+
+template <typename R>
+void FactorStore<R>::Factor() {
+    if (!layout_) BuildLayout();
+    CUDA_CHECK(cudaMemsetAsync(status_.p, 0, sizeof(int), h_.stream_));
+    for (int& c : slotHolds_) c = -1;  // the velocity changed: slots are stale
+    refactors_ = 0;
+    // replay the recorded factorization while the scratch has not moved
+    bool replay = !program_.empty();
+    for (const auto& pg : program_)
+        replay = replay && pg->arena == h_.Scratch(0) && pg->arenaBytes <= h_.ScratchBytes();
+    if (!replay) {
+        program_.clear();
+        const PanelGeometry& g = an_.geom;
+        std::vector<int> res;
+        for (int p = 0; p < g.numPanels; ++p)
+            if (resident_[p]) res.push_back(p);
+        // groups of resident panels whose transients fit in 80% of the free
+        // memory (the scratch counts as free: it is reused)
+        size_t freeB = 0, totalB = 0;
+        CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
+        const int64_t budget = (int64_t)(0.8 * ((double)freeB + (double)h_.ScratchBytes()));
+        int groupSize = std::max<int>(1, (int)res.size());
+        auto slice = [&](size_t i0, int n) {
+            return std::vector<int>(res.begin() + i0, res.begin() + std::min(res.size(), i0 + n));
+        };
+        auto maxTransient = [&](int n) {
+            int64_t m = 0;
+            for (size_t i0 = 0; i0 < res.size(); i0 += n) m = std::max(m, TransientBytes(slice(i0, n)));
+            return m;
+        };
+        while (groupSize > 1 && maxTransient(groupSize) > budget) groupSize = (groupSize + 1) / 2;
+        const int64_t need = res.empty() ? 0 : maxTransient(groupSize);
+        unsigned char* arena = static_cast<unsigned char*>(h_.Scratch(need));
+        for (size_t i0 = 0; i0 < res.size(); i0 += groupSize)
+            program_.push_back(FactorGroup(slice(i0, groupSize), arena, need));
+    }
+    for (auto& pg : program_) RunProgram(*pg, false);
+    CUDA_CHECK(cudaStreamSynchronize(h_.stream_));
     CheckPivots();
+}
+
+template <typename R>
+void FactorStore<R>::EnsurePanel(int p) {
+    if (resident_[p]) return;
+    const int c = an_.geom.Class(p);
+    if (slotHolds_[c] == p) return;
+    RunProgram(*recompute_[p], false);
+    slotHolds_[c] = p;
+    ++refactors_;
 }
 
 template <typename R>
@@ -370,20 +564,23 @@ void FactorStore<R>::CheckPivots() {
 }
 
 template <typename R>
-void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& all, bool keep) {
+std::unique_ptr<typename FactorStore<R>::FactorProgram> FactorStore<R>::FactorGroup(const std::vector<int>& panels,
+                                                                                   unsigned char* arenaBase,
+                                                                                   size_t arenaBytes) {
     const PanelGeometry& g = an_.geom;
     const XYTree& tree = an_.tree;
     const int nd = (int)depthNodes_.size();
+    const int ng = (int)panels.size();
     cudaStream_t st = h_.stream_;
     // per-depth transient layout
     std::vector<int64_t> Lsz(nd, 0), Usz(nd, 0), Tsz(nd, 0);
-    std::vector<int64_t> Lpos((size_t)(p1 - p0) * nn_), Upos((size_t)(p1 - p0) * nn_), Tpos((size_t)(p1 - p0) * nn_);
+    std::vector<int64_t> Lpos((size_t)ng * nn_), Upos((size_t)ng * nn_), Tpos((size_t)ng * nn_);
     for (int d = 0; d < nd; ++d)
-        for (int p = p0; p < p1; ++p) {
-            const ClassStructure& cs = an_.cls[g.Class(p)];
+        for (int gi = 0; gi < ng; ++gi) {
+            const ClassStructure& cs = an_.cls[g.Class(panels[gi])];
             for (int t : depthNodes_[d]) {
                 const int64_t s = cs.size[t], u = cs.usize[t];
-                const size_t i = (size_t)(p - p0) * nn_ + t;
+                const size_t i = (size_t)gi * nn_ + t;
                 Lpos[i] = Lsz[d]; Lsz[d] += (s + u) * s;
                 Upos[i] = Usz[d]; Usz[d] += u * u;
                 Tpos[i] = Tsz[d]; Tsz[d] += (s / 2 + 1) * (s / 2 + 1) * 2;
@@ -395,23 +592,34 @@ void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& al
         lm = std::max(lm, Lsz[d]);
         tm = std::max(tm, Tsz[d]);
     }
+    if ((size_t)(ua + ub + lm + tm) * sizeof(cpx<R>) > arenaBytes)
+        throw PspError(kRuntimeError, "factorization transients exceed their arena");
     std::unique_ptr<FactorProgram> pgHolder(new FactorProgram);
     FactorProgram& pg = *pgHolder;
-    DeviceBuffer& arena = pg.arena;
-    arena.Allocate((ua + ub + lm + tm) * sizeof(cpx<R>));
-    cpx<R>* UA = arena.as<cpx<R>>();
+    pg.arena = arenaBase;
+    pg.arenaBytes = arenaBytes;
+    cpx<R>* UA = reinterpret_cast<cpx<R>*>(arenaBase);
     cpx<R>* UB = UA + ua;
     cpx<R>* Lb = UB + ub;
     cpx<R>* Tb = Lb + lm;
+    // the group's fronts, indexed gi * nn_ + t (parents likewise)
+    std::vector<FactorFront<R>> all((size_t)ng * nn_);
+    for (int gi = 0; gi < ng; ++gi)
+        for (int t = 0; t < nn_; ++t) {
+            FactorFront<R>& f = all[(size_t)gi * nn_ + t];
+            f = fronts_[(size_t)panels[gi] * nn_ + t];
+            f.parent = tree.nodes[t].parent < 0 ? -1 : gi * nn_ + tree.nodes[t].parent;
+        }
     for (int d = 0; d < nd; ++d)
-        for (int p = p0; p < p1; ++p)
+        for (int gi = 0; gi < ng; ++gi)
             for (int t : depthNodes_[d]) {
-                const size_t i = (size_t)(p - p0) * nn_ + t;
-                FactorFront<R>& f = all[(size_t)p * nn_ + t];
+                const size_t i = (size_t)gi * nn_ + t;
+                FactorFront<R>& f = all[i];
                 f.L = Lb + Lpos[i];
                 f.U = (d % 2 ? UB : UA) + Upos[i];
                 f.T = Tb + Tpos[i];
             }
+    const char* arenaP = reinterpret_cast<const char*>(arenaBase);
 
     TaskArena& arenaTasks = pg.tasks;
     pg.frontsOff = arenaTasks.Push(all);
@@ -452,20 +660,20 @@ void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& al
     for (int d = nd - 1; d >= 0; --d) {
         std::vector<int> list;
         int maxS = 0;
-        for (int p = p0; p < p1; ++p)
+        for (int gi = 0; gi < ng; ++gi)
             for (int t : depthNodes_[d]) {
-                list.push_back(p * nn_ + t);
-                maxS = std::max(maxS, all[(size_t)p * nn_ + t].s);
+                list.push_back(gi * nn_ + t);
+                maxS = std::max(maxS, all[(size_t)gi * nn_ + t].s);
             }
         if (list.empty()) continue;
         // zero this depth's frontal columns and update matrices
         {
             Step s;
             s.kind = Step::kMemset;
-            s.a = (size_t)((char*)Lb - (char*)arena.p);
+            s.a = (size_t)((const char*)Lb - arenaP);
             s.bytes = Lsz[d] * sizeof(cpx<R>);
             steps.push_back(s);
-            s.a = (size_t)((char*)(d % 2 ? UB : UA) - (char*)arena.p);
+            s.a = (size_t)((const char*)(d % 2 ? UB : UA) - arenaP);
             s.bytes = Usz[d] * sizeof(cpx<R>);
             steps.push_back(s);
         }
@@ -576,20 +784,18 @@ void FactorStore<R>::FactorGroup(int p0, int p1, std::vector<FactorFront<R>>& al
         pushGemm();
     }
     arenaTasks.Upload(st);
-    RunProgram(pg);
-    if (keep) program_.push_back(std::move(pgHolder));
+    return pgHolder;
 }
 
 template <typename R>
-void FactorStore<R>::RunProgram(FactorProgram& pg) {
+void FactorStore<R>::RunProgram(FactorProgram& pg, bool sync) {
     cudaStream_t st = h_.stream_;
-    const DeviceBuffer& arena = pg.arena;
     const TaskArena& arenaTasks = pg.tasks;
     const FactorFront<R>* dFronts = arenaTasks.template At<FactorFront<R>>(pg.frontsOff);
     for (const Step& s : pg.steps) {
         switch (s.kind) {
             case Step::kMemset:
-                if (s.bytes) CUDA_CHECK(cudaMemsetAsync((char*)arena.p + s.a, 0, s.bytes, st));
+                if (s.bytes) CUDA_CHECK(cudaMemsetAsync(pg.arena + s.a, 0, s.bytes, st));
                 break;
             case Step::kAssemble: {
                 ProfScope ps(st, kProfAssemble);
@@ -622,7 +828,7 @@ void FactorStore<R>::RunProgram(FactorProgram& pg) {
             }
         }
     }
-    CUDA_CHECK(cudaStreamSynchronize(st));
+    if (sync) CUDA_CHECK(cudaStreamSynchronize(st));
 }
 
 template <typename R>
@@ -671,8 +877,8 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
         for (int t = 0; t < nn_; ++t) {
             SweepFront<R>& f = fr[t];
             const XYNode& node = tree.nodes[t];
-            f.G = G_.as<cpx<R>>() + gOff_[(size_t)p * nn_ + t];
-            f.D = D_.as<cpx<R>>() + dOff_[(size_t)p * nn_ + t];
+            f.G = gPtr_[(size_t)p * nn_ + t];
+            f.D = dPtr_[(size_t)p * nn_ + t];
             f.Rb = P.Rb.template as<cpx<R>>() + rOff[c][t];
             f.parentRb = node.parent >= 0 ? P.Rb.template as<cpx<R>>() + rOff[c][node.parent] : nullptr;
             f.Y = P.Y.template as<cpx<R>>() + yOff[c][t];
@@ -870,8 +1076,10 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
                 // no two tuning runs time each other's launches
                 std::lock_guard<std::mutex> tuning(gTuneMutex);
                 lookup();
-                if (routes.empty()) {
-                    Autotune(P);
+                if (routes.empty() && Autotune(P)) {
+                    // only measured choices are shared: a handle that could
+                    // not time its candidates keeps the default tiling, and a
+                    // later one with room tunes
                     for (const ClassPlan& cp : P.cplan) {
                         routes.insert(routes.end(), cp.fSel.begin(), cp.fSel.end());
                         routes.insert(routes.end(), cp.bSel.begin(), cp.bSel.end());
@@ -882,8 +1090,8 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             }
             size_t i = 0;
             for (ClassPlan& cp : P.cplan) {
-                for (int& r : cp.fSel) r = routes[i++];
-                for (int& r : cp.bSel) r = routes[i++];
+                for (int& r : cp.fSel) r = routes.empty() ? 0 : routes[i++];
+                for (int& r : cp.bSel) r = routes.empty() ? 0 : routes[i++];
             }
         }
     }
@@ -891,7 +1099,7 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
 }
 
 template <typename R>
-void FactorStore<R>::Autotune(SolvePlan& P) {
+bool FactorStore<R>::Autotune(SolvePlan& P) {
     const PanelGeometry& g = an_.geom;
     const int nd = (int)depthNodes_.size(), k = P.k;
     const int reps = 2;
@@ -901,7 +1109,7 @@ void FactorStore<R>::Autotune(SolvePlan& P) {
     } catch (const PspError& e) {
         if (e.code != kOutOfMemory) throw;
         cudaGetLastError();  // no room for timing runs: keep the default tiling
-        return;
+        return false;
     }
     CUDA_CHECK(cudaMemsetAsync(scratch.p, 0, scratch.bytes, h_.stream_));
     TuneEvents te;
@@ -973,11 +1181,13 @@ void FactorStore<R>::Autotune(SolvePlan& P) {
         throw;
     }
     for (cudaEvent_t e : te.ev) CUDA_CHECK(cudaEventDestroy(e));
+    return true;
 }
 
 template <typename R>
 void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc) {
     SolvePlan& P = Plan(k);
+    EnsurePanel(p);
     const PanelGeometry& g = an_.geom;
     const int c = g.Class(p);
     const ClassPlan& cp = P.cplan[c];
@@ -1055,7 +1265,8 @@ template <typename R>
 void FactorStore<R>::Sweep(z64* B, int ldk, int k, bool useGraph) {
     Profiler* prof = CurrentProfiler();
     const bool profiling = prof && prof->enabled;
-    if (!useGraph || profiling) {
+    // recomputed panels factor inside the sweep (host-side slot tracking): eager
+    if (!useGraph || profiling || !AllResident()) {
         ProfScope ps(h_.stream_, kProfSweep, SweepFlops(k), SweepBytes(k));
         SweepEager(B, ldk, k);
         return;
@@ -1066,6 +1277,10 @@ void FactorStore<R>::Sweep(z64* B, int ldk, int k, bool useGraph) {
             CUDA_CHECK(cudaGraphLaunch(g.exec, h_.stream_));
             return;
         }
+    if (graphs_.size() >= 8) {  // graphs of earlier work vectors (the scratch moved)
+        CUDA_CHECK(cudaGraphExecDestroy(graphs_.front().exec));
+        graphs_.erase(graphs_.begin());
+    }
     cudaGraph_t graph;
     CUDA_CHECK(cudaStreamBeginCapture(h_.stream_, cudaStreamCaptureModeThreadLocal));
     SweepEager(B, ldk, k);
@@ -1075,6 +1290,35 @@ void FactorStore<R>::Sweep(z64* B, int ldk, int k, bool useGraph) {
     CUDA_CHECK(cudaGraphDestroy(graph));
     graphs_.push_back(g);
     CUDA_CHECK(cudaGraphLaunch(g.exec, h_.stream_));
+}
+
+template <typename R>
+double FactorStore<R>::PlanBytesPerRhs() const {
+    double best = 0;
+    for (int c = 0; c < 3; ++c) {
+        if (!an_.classUsed[c]) continue;
+        const ClassStructure& cs = an_.cls[c];
+        double e = cs.nSub;
+        for (size_t t = 0; t < cs.size.size(); ++t) e += 3.0 * (cs.size[t] + cs.usize[t]) + cs.size[t] + (cs.size[t] + cs.usize[t]);
+        best = std::max(best, e);
+    }
+    return best * sizeof(cpx<R>);
+}
+
+template <typename R>
+void FactorStore<R>::DropPlansExcept(int k) {
+    for (size_t i = 0; i < graphs_.size();) {
+        if (graphs_[i].k != k) {
+            CUDA_CHECK(cudaGraphExecDestroy(graphs_[i].exec));
+            graphs_.erase(graphs_.begin() + i);
+        } else {
+            ++i;
+        }
+    }
+    for (size_t i = 0; i < plans_.size();) {
+        if (plans_[i]->k != k) plans_.erase(plans_.begin() + i);
+        else ++i;
+    }
 }
 
 // Algorithmic work of one sweep: every panel but the top one is solved twice.
@@ -1234,7 +1478,28 @@ void Helmholtz::Initialize(const double* velocity, bool devicePtr, int panelSche
 void Helmholtz::Finalize() {
     f64_.reset();
     f32_.reset();
+    pool_.Release();
     initialized_ = false;
+}
+
+void* Helmholtz::Scratch(size_t bytes) {
+    if (bytes > pool_.bytes) {
+        pool_.Release();
+        pool_.Allocate(bytes);
+    }
+    return pool_.p;
+}
+
+int Helmholtz::ResidentPanels() const {
+    if (f64_) return f64_->ResidentPanels();
+    if (f32_) return f32_->ResidentPanels();
+    return 0;
+}
+
+int64_t Helmholtz::Refactorizations() const {
+    if (f64_) return f64_->Refactorizations();
+    if (f32_) return f32_->Refactorizations();
+    return 0;
 }
 
 int64_t Helmholtz::factorBytes() const {
@@ -1274,6 +1539,7 @@ void Helmholtz::Precondition(z64* B, int k, bool useGraph) {
 
 void Helmholtz::CheckSweepStatus() {
     const int st = f64_ ? f64_->ReadStatus() : (f32_ ? f32_->ReadStatus() : 0);
+    if (st & 1) throw PspError(kRuntimeError, "zero or non-finite pivot in a recomputed panel factorization");
     if (st & 2) throw PspError(kRuntimeError, "a tensor-core pipeline wait timed out in the sweep");
 }
 
@@ -1319,19 +1585,25 @@ void Helmholtz::GradientDevice(const z64* U, const z64* Z, int k, double* grad, 
     CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 
-void Helmholtz::EnsureWorkspace(int k, int m) {
-    if (wsK_ == k && wsM_ == m) return;
-    const int64_t nk = NumUnknowns() * k;
-    dX_.Allocate(nk * sizeof(z64));
-    dX0_.Allocate(nk * sizeof(z64));
-    dW_.Allocate(nk * sizeof(z64));
-    dB_.Allocate(nk * sizeof(z64));
-    dV_.Allocate((size_t)m * nk * sizeof(z64));
-    dPartial_.Allocate((size_t)ReduceBlocks(NumUnknowns(), k) * k * sizeof(z64));
-    dScal_.Allocate((size_t)(2 * k) * sizeof(double) + (size_t)(m + 1) * k * sizeof(z64));
-    dY_.Allocate((size_t)m * k * sizeof(z64));
-    wsK_ = k;
-    wsM_ = m;
+void Helmholtz::EnsureWorkspace(int k, int m, bool withCols) {
+    const size_t nk = (size_t)NumUnknowns() * k;
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t vec = al(nk * sizeof(z64));
+    const size_t partial = al((size_t)ReduceBlocks(NumUnknowns(), k) * k * sizeof(z64));
+    const size_t scal = al((size_t)(2 * k) * sizeof(double) + (size_t)(m + 1) * k * sizeof(z64));
+    const size_t ybytes = al((size_t)m * k * sizeof(z64));
+    const size_t total = vec * (4 + m + (withCols ? 1 : 0)) + partial + scal + ybytes;
+    unsigned char* p = static_cast<unsigned char*>(Scratch(total));
+    auto take = [&](size_t b) { unsigned char* q = p; p += b; return q; };
+    wsCols_ = withCols ? reinterpret_cast<z64*>(take(vec)) : nullptr;
+    wsX_ = reinterpret_cast<z64*>(take(vec));
+    wsX0_ = reinterpret_cast<z64*>(take(vec));
+    wsW_ = reinterpret_cast<z64*>(take(vec));
+    wsB_ = reinterpret_cast<z64*>(take(vec));
+    wsV_ = reinterpret_cast<z64*>(take(vec * m));
+    wsPartial_ = take(partial);
+    wsScal_ = take(scal);
+    wsY_ = reinterpret_cast<z64*>(take(ybytes));
 }
 
 namespace {
@@ -1356,20 +1628,39 @@ bool AnyNaN(const std::vector<double>& v) {
 
 }  // namespace
 
+double Helmholtz::GmresBytesPerRhs(int m) const {
+    // V (m vectors), x, x0, w, b and a block's copy of its columns, the
+    // solve plan's work vectors and the sweep autotuner's scratch
+    double plan = 0;
+    if (f64_) plan = f64_->PlanBytesPerRhs();
+    if (f32_) plan = f32_->PlanBytesPerRhs();
+    return (double)NumUnknowns() * sizeof(z64) * (m + 6) + plan;
+}
+
 int Helmholtz::GmresBlockWidth(int k, int m) {
-    int kb = k;
-    if (const char* env = std::getenv("PSP_B200_MAX_RHS_BLOCK")) {
-        const int cap = std::atoi(env);
-        if (cap > 0) kb = std::min(kb, cap);
-    }
+    int cap = k;
+    const long long env = EnvInt("PSP_B200_MAX_RHS_BLOCK", 0);
+    if (env > 0) cap = (int)std::min<long long>(cap, env);
     size_t freeB = 0, totalB = 0;
     CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
-    // the workspace held now is released before a different width is allocated
-    const double held = wsK_ > 0 ? (double)NumUnknowns() * wsK_ * sizeof(z64) * (wsM_ + 4) : 0.0;
-    // V (m vectors), x, x0, w, b and a block's copy of its columns
-    const double perRhs = (double)NumUnknowns() * sizeof(z64) * (m + 6);
-    const double fit = std::floor(0.85 * ((double)freeB + held) / perRhs);
-    if (fit >= 1 && fit < kb) kb = (int)fit;
+    // the scratch is reused for the workspace; the plan of the current width
+    // (when built) is already counted as used memory
+    const double avail = (double)freeB + (double)pool_.bytes - 0.5e9;
+    const double perRhs = GmresBytesPerRhs(m);
+    const double fitD = std::floor(0.95 * avail / perRhs);
+    if (fitD < 1)
+        throw PspError(kOutOfMemory, "the GMRES workspace of one right-hand side (" +
+                                         std::to_string(perRhs / 1e9) + " GB at restart " + std::to_string(m) +
+                                         ") does not fit in the " + std::to_string(avail / 1e9) +
+                                         " GB of device memory left beside the factors");
+    const int fit = (int)std::min<double>(fitD, cap);
+    const int nb = (k + fit - 1) / fit;
+    int kb = (k + nb - 1) / nb;
+    // whole 16-column sweep tiles when that still fits
+    if (kb > 16 && kb % 16) {
+        const int up = (kb + 15) / 16 * 16;
+        if (up <= fit && up < k) kb = up;
+    }
     return std::max(1, kb);
 }
 
@@ -1380,6 +1671,7 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     CUDA_CHECK(cudaSetDevice(device_));
     const int kb = GmresBlockWidth(k, m);
     if (kb >= k) {
+        EnsureWorkspace(k, m, false);
         SolveBlock(B, k, m, relTol, stats);
         return;
     }
@@ -1389,13 +1681,12 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     S = SolveStats();
     S.converged = 1;
     const int64_t N = NumUnknowns();
-    if (wsK_ != kb || wsM_ != m) {
-        // the blocks allocate their own width; free the old one first
-        for (DeviceBuffer* b : {&dX_, &dX0_, &dW_, &dB_, &dV_, &dPartial_, &dScal_, &dY_}) b->Release();
-        wsK_ = wsM_ = -1;
-    }
-    DeviceBuffer cols;
-    cols.Allocate((size_t)N * kb * sizeof(z64));
+    // blocks of equal width kb (one solve plan); a short last block is
+    // padded with copies of its last column, whose results are dropped
+    if (f64_) f64_->DropPlansExcept(RhsBlockWidth(kb));
+    if (f32_) f32_->DropPlansExcept(RhsBlockWidth(kb));
+    EnsureWorkspace(kb, m, true);
+    z64* cols = wsCols_;
     const std::string viewBase = viewIterates_;
     std::vector<std::vector<Cd>> ritzPerRhs;
     int ritzCount = 0;
@@ -1406,14 +1697,18 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
     } restore{*this, viewBase};
     for (int c0 = 0; c0 < k; c0 += kb) {
         const int w = std::min(kb, k - c0);
-        // columns [c0, c0 + w) of the [N][k] grid as a contiguous [N][w] grid
-        CUDA_CHECK(cudaMemcpy2DAsync(cols.p, w * sizeof(z64), B + c0, k * sizeof(z64), w * sizeof(z64), N,
+        // columns [c0, c0 + w) of the [N][k] grid as a contiguous [N][kb] grid
+        CUDA_CHECK(cudaMemcpy2DAsync(cols, kb * sizeof(z64), B + c0, k * sizeof(z64), w * sizeof(z64), N,
                                      cudaMemcpyDeviceToDevice, stream_));
+        for (int c = w; c < kb; ++c)
+            CUDA_CHECK(cudaMemcpy2DAsync(cols + c, kb * sizeof(z64), B + c0 + w - 1, k * sizeof(z64), sizeof(z64), N,
+                                         cudaMemcpyDeviceToDevice, stream_));
         if (!viewBase.empty()) viewIterates_ = viewBase + "_rhs" + std::to_string(c0);
         ritzRhsOffset_ = c0;
         SolveStats s;
-        SolveBlock(cols.as<z64>(), w, m, relTol, &s);
-        CUDA_CHECK(cudaMemcpy2DAsync(B + c0, k * sizeof(z64), cols.p, w * sizeof(z64), w * sizeof(z64), N,
+        EnsureWorkspace(kb, m, true);
+        SolveBlock(cols, kb, m, relTol, &s);
+        CUDA_CHECK(cudaMemcpy2DAsync(B + c0, k * sizeof(z64), cols, kb * sizeof(z64), w * sizeof(z64), N,
                                      cudaMemcpyDeviceToDevice, stream_));
         S.iterations = std::max(S.iterations, s.iterations);
         S.converged = S.converged && s.converged;
@@ -1426,7 +1721,7 @@ void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* sta
         if (S.history.size() < s.history.size()) S.history.resize(s.history.size(), 0.0);
         for (size_t i = 0; i < s.history.size(); ++i) S.history[i] = std::max(S.history[i], s.history[i]);
         if (ritzK_ > 0) {
-            for (int r = 0; r < ritzK_; ++r)
+            for (int r = 0; r < w; ++r)
                 ritzPerRhs.emplace_back(ritz_.begin() + (size_t)r * ritzCount_,
                                         ritz_.begin() + (size_t)(r + 1) * ritzCount_);
             ritzCount = std::max(ritzCount, ritzCount_);
@@ -1451,26 +1746,33 @@ void Helmholtz::SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stat
     if (m < 1) throw PspError(kLogicError, "GMRES restart length must be positive");
     CUDA_CHECK(cudaSetDevice(device_));
     const auto tStart = std::chrono::steady_clock::now();
-    EnsureWorkspace(k, m);
     SolveStats local;
     SolveStats& S = stats ? *stats : local;
     S = SolveStats();
     const int64_t N = NumUnknowns(), nk = N * k;
     cudaStream_t st = stream_;
-    z64* x = dX_.as<z64>();
-    z64* x0 = dX0_.as<z64>();
-    z64* w = dW_.as<z64>();
-    z64* b = dB_.as<z64>();
-    z64* V = dV_.as<z64>();
-    double* dNorm = dScal_.as<double>();
+    z64* x = wsX_;
+    z64* x0 = wsX0_;
+    z64* w = wsW_;
+    z64* b = wsB_;
+    z64* V = wsV_;
+    double* dNorm = static_cast<double*>(wsScal_);
     double* dDelta = dNorm + k;
     z64* dH = reinterpret_cast<z64*>(dDelta + k);
-    z64* dY = dY_.as<z64>();
+    z64* dY = wsY_;
+    double* partialR = static_cast<double*>(wsPartial_);
+    z64* partialC = static_cast<z64*>(wsPartial_);
     const int nblk = ReduceBlocks(N, k);
     const double* vel = dVel_.as<double>();
+    // per-kernel profiling (when on) of the GMRES vector kernels: algorithmic
+    // bytes = the [N][k] vectors each launch reads and writes
+    const double vb = 16.0 * (double)nk;
     auto norms = [&](const z64* v, double* out) {
-        LaunchNormsPartial(v, N, k, dPartial_.as<double>(), st);
-        LaunchSumPartialReal(dPartial_.as<double>(), nblk, k, out, 1, st);
+        {
+            ProfScope ps(st, kProfVector, 4.0 * nk, vb);
+            LaunchNormsPartial(v, N, k, partialR, st);
+        }
+        LaunchSumPartialReal(partialR, nblk, k, out, 1, st);
     };
     auto fetch = [&](void* dst, const void* src, size_t bytes) {
         CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
@@ -1544,20 +1846,31 @@ void Helmholtz::SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stat
         fetch(beta.data(), dNorm, k * sizeof(double));
         CUDA_CHECK(cudaStreamSynchronize(st));
         if (AnyNaN(beta)) throw PspError(kRuntimeError, "beta list had a NaN");
-        LaunchScaleColumns(w, dNorm, V, N, k, st);
+        {
+            ProfScope ps(st, kProfVector, 2.0 * nk, 2 * vb);
+            LaunchScaleColumns(w, dNorm, V, N, k, st);
+        }
         std::fill(z.begin(), z.end(), Cd(0));
         for (int r = 0; r < k; ++r) z[(size_t)r * (m + 1)] = beta[r];
         for (int j = 0; j < m; ++j) {
-            timed(kProfStencil, mvFlops, mvBytes,
-                  [&] { LaunchHelmholtzApply(V + (size_t)j * nk, w, nullptr, vel, sp_, k, st); });
+            timed(kProfStencil, mvFlops, mvBytes, [&] {
+                ProfScope ps(st, kProfStencil, mvFlops, mvBytes);
+                LaunchHelmholtzApply(V + (size_t)j * nk, w, nullptr, vel, sp_, k, st);
+            });
             precond();
             phases.Begin(st);
             for (int i = 0; i <= j; ++i) {
-                LaunchMgsStep(w, i > 0 ? V + (size_t)(i - 1) * nk : nullptr, i > 0 ? dH + (size_t)(i - 1) * k : nullptr,
-                              V + (size_t)i * nk, N, k, dPartial_.as<z64>(), st);
-                LaunchSumPartialComplex(dPartial_.as<z64>(), nblk, k, dH + (size_t)i * k, st);
+                {
+                    ProfScope ps(st, kProfVector, (i > 0 ? 16.0 : 8.0) * nk, (i > 0 ? 4 : 2) * vb);
+                    LaunchMgsStep(w, i > 0 ? V + (size_t)(i - 1) * nk : nullptr,
+                                  i > 0 ? dH + (size_t)(i - 1) * k : nullptr, V + (size_t)i * nk, N, k, partialC, st);
+                }
+                LaunchSumPartialComplex(partialC, nblk, k, dH + (size_t)i * k, st);
             }
-            LaunchAxpyColumns(w, V + (size_t)j * nk, dH + (size_t)j * k, N, k, st);
+            {
+                ProfScope ps(st, kProfVector, 8.0 * nk, 3 * vb);
+                LaunchAxpyColumns(w, V + (size_t)j * nk, dH + (size_t)j * k, N, k, st);
+            }
             norms(w, dDelta);
             phases.End(st, kProfVector, 8.0 * 2 * (j + 1) * nk, 16.0 * (3 * (j + 1) + 2) * nk);
             hcol.resize((size_t)(j + 1) * k);
@@ -1583,7 +1896,10 @@ void Helmholtz::SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stat
                     if (j + 1 != m) Hr[(size_t)j * m + j + 1] = delta[r];
                 }
             phases.Begin(st);
-            if (j + 1 != m) LaunchScaleColumns(w, dDelta, V + (size_t)(j + 1) * nk, N, k, st);
+            if (j + 1 != m) {
+                ProfScope ps(st, kProfVector, 2.0 * nk, 2 * vb);
+                LaunchScaleColumns(w, dDelta, V + (size_t)(j + 1) * nk, N, k, st);
+            }
             for (int r = 0; r < k; ++r) {
                 Cd* Hr = &H[(size_t)r * m * m];
                 for (int i = 0; i <= j; ++i) Hr[(size_t)j * m + i] = Cd(hcol[(size_t)i * k + r]);
@@ -1614,9 +1930,15 @@ void Helmholtz::SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stat
                 }
             }
             CUDA_CHECK(cudaMemcpyAsync(dY, y.data(), (size_t)(j + 1) * k * sizeof(z64), cudaMemcpyHostToDevice, st));
-            LaunchCombine(x0, V, nk, dY, j + 1, x, N, k, st);
+            {
+                ProfScope ps(st, kProfVector, 8.0 * (j + 1) * nk, (j + 3) * vb);
+                LaunchCombine(x0, V, nk, dY, j + 1, x, N, k, st);
+            }
             phases.End(st, kProfVector, 8.0 * (j + 1) * nk, 16.0 * (j + 3) * nk);
-            timed(kProfStencil, mvFlops, mvBytes + 16.0 * nk, [&] { LaunchHelmholtzApply(x, w, b, vel, sp_, k, st); });
+            timed(kProfStencil, mvFlops, mvBytes + 16.0 * nk, [&] {
+                ProfScope ps(st, kProfStencil, mvFlops, mvBytes + 16.0 * nk);
+                LaunchHelmholtzApply(x, w, b, vel, sp_, k, st);
+            });
             norms(w, dNorm);
             fetch(resid.data(), dNorm, k * sizeof(double));
             CUDA_CHECK(cudaStreamSynchronize(st));

@@ -123,6 +123,26 @@ public:
     // Sweep algorithmic flops/bytes for k right-hand sides (0 before Initialize).
     double SweepFlops(int k) const;
     double SweepBytes(int k) const;
+    // Panels whose factors stay resident in device memory; the others are
+    // re-factored into a per-class slot whenever a sweep reaches them.
+    int ResidentPanels() const;
+    // Panel factorizations run by sweeps since Initialize (recomputed panels).
+    int64_t Refactorizations() const;
+
+    // Right-hand sides per GMRES block a Solve of k sides with restart m
+    // would use now (k when they all fit).
+    int SolveBlockWidth(int k, int m) {
+        if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+        if (k < 1 || m < 1) throw PspError(kLogicError, "need k >= 1 and m >= 1");
+        return GmresBlockWidth(k, m);
+    }
+
+    // Device scratch shared by the factorization transients (Initialize)
+    // and the GMRES workspace (Solve), which are never live at the same
+    // time.  Grows to `bytes` (its contents and earlier pointers into it
+    // are lost when it does) and returns its base.
+    void* Scratch(size_t bytes);
+    size_t ScratchBytes() const { return pool_.bytes; }
 
     // Device tables shared with the factor stores.
     StencilParams sp_{};
@@ -139,12 +159,19 @@ public:
 private:
     void BuildTables();
     void Precondition(z64* B, int k, bool useGraph);
-    void EnsureWorkspace(int k, int m);
+    // Carves the GMRES workspace for k right-hand sides and restart m (and,
+    // for blocked solves, a k-wide copy of a block's columns) from Scratch.
+    void EnsureWorkspace(int k, int m, bool withCols);
     void CheckSweepStatus();
     // GMRES over all k columns of B at once (the reference's form).
     void SolveBlock(z64* B, int k, int m, double relTol, SolveStats* stats);
-    // Right-hand sides per GMRES block for k sides and restart m.
+    // Right-hand sides per GMRES block for k sides and restart m: the
+    // widest that fits in device memory (or the environment's cap), made
+    // equal across blocks and, from 16 up, a multiple of 16 when that still
+    // fits.  Throws out-of-memory when not even one right-hand side fits.
     int GmresBlockWidth(int k, int m);
+    // Device bytes one right-hand side of a GMRES block needs with restart m.
+    double GmresBytesPerRhs(int m) const;
 
     Profiler prof_;
     bool initialized_ = false;
@@ -156,9 +183,12 @@ private:
     double setupSeconds_ = 0;
     std::unique_ptr<FactorStore<double>> f64_;
     std::unique_ptr<FactorStore<float>> f32_;
-    // GMRES workspace
-    int wsK_ = -1, wsM_ = -1;
-    DeviceBuffer dX_, dX0_, dW_, dB_, dV_, dPartial_, dScal_, dY_;
+    DeviceBuffer pool_;
+    // GMRES workspace, carved from pool_ by EnsureWorkspace
+    z64 *wsX_ = nullptr, *wsX0_ = nullptr, *wsW_ = nullptr, *wsB_ = nullptr, *wsV_ = nullptr;
+    z64 *wsCols_ = nullptr, *wsY_ = nullptr;
+    void* wsPartial_ = nullptr;
+    void* wsScal_ = nullptr;
 };
 
 }  // namespace psp_b200

@@ -24,24 +24,89 @@ SIGMA = 1.5  # UnitCube default --sigma (tests/UnitCube.cpp:28)
 
 
 class Workload:
+    """A velocity model and its right-hand sides.  ``rhs`` is either the
+    dense (nz, ny, nx, k) complex128 array or a :class:`SeparableSources`,
+    in which case the dense array is built on first use (``rhs``) and can be
+    built directly on a CUDA device (``rhs_torch``) without a host copy."""
+
     def __init__(self, name, disc, velocity, rhs, pml, interior, meta):
         self.name = name
         self.disc = disc
         self.velocity = velocity      # (nz, ny, nx) float64
-        self.rhs = rhs                # (nz, ny, nx, k) complex128
+        self._rhs = rhs
         self.pml = pml
         self.interior = interior
         self.meta = meta
 
     @property
+    def rhs(self):
+        """(nz, ny, nx, k) complex128."""
+        if isinstance(self._rhs, SeparableSources):
+            self._rhs = self._rhs.dense()
+        return self._rhs
+
+    @property
     def k(self):
-        return self.rhs.shape[-1]
+        return self._rhs.k if isinstance(self._rhs, SeparableSources) else self._rhs.shape[-1]
+
+    def rhs_torch(self, device, out=None, cols=None):
+        """The right-hand sides (or the sources ``cols``, a range) as a CUDA
+        complex128 tensor of nx*ny*nz*len(cols) entries (natural order,
+        interleaved per point), written into ``out`` when given."""
+        import torch
+        if isinstance(self._rhs, SeparableSources):
+            return self._rhs.torch(device, out, cols)
+        a = self._rhs if cols is None else self._rhs[..., cols]
+        t = torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to(device)
+        if out is None:
+            return t
+        out.copy_(t)
+        return out
+
+    def rhs_host(self, cols=None):
+        """The right-hand sides (or the sources ``cols``) as a C-contiguous
+        (nz, ny, nx, len(cols)) complex128 array."""
+        if isinstance(self._rhs, SeparableSources):
+            return self._rhs.dense(cols)
+        return np.ascontiguousarray(self._rhs if cols is None else self._rhs[..., cols])
 
     def velocity_grid(self):
         return DistUniformGrid(self.disc.nx, self.disc.ny, self.disc.nz, 1, np.float64, self.velocity)
 
     def rhs_grid(self):
         return DistUniformGrid(self.disc.nx, self.disc.ny, self.disc.nz, self.k, np.complex128, self.rhs.copy())
+
+
+class SeparableSources:
+    """k point sources whose fields are products gz(z) gy(y) gx(x) (the
+    Gaussians of width 2h the reference's drivers use, UnitCube.cpp:485-542),
+    kept as their 1-D factors: g[axis][r] is source r's factor along that
+    axis, the field is -gz gy gx."""
+
+    def __init__(self, gx, gy, gz):
+        self.gx, self.gy, self.gz = (np.asarray(a, dtype=np.float64) for a in (gx, gy, gz))
+        self.k = self.gx.shape[0]
+
+    def dense(self, cols=None):
+        cols = range(self.k) if cols is None else cols
+        out = np.empty((self.gz.shape[1], self.gy.shape[1], self.gx.shape[1], len(cols)), dtype=np.complex128)
+        for j, r in enumerate(cols):
+            out[..., j] = -(self.gz[r][:, None, None] * self.gy[r][None, :, None] * self.gx[r][None, None, :])
+        return out
+
+    def torch(self, device, out=None, cols=None):
+        import torch
+        cols = list(range(self.k) if cols is None else cols)
+        gx, gy, gz = (torch.from_numpy(a[cols].T.copy()).to(device) for a in (self.gx, self.gy, self.gz))
+        nz, ny, nx, kk = gz.shape[0], gy.shape[0], gx.shape[0], len(cols)
+        if out is None:
+            out = torch.empty(nz * ny * nx * kk, dtype=torch.complex128, device=device)
+        view = torch.view_as_real(out.view(nz, ny, nx, kk))
+        view[..., 1].zero_()
+        for z in range(nz):  # -(gz gy) gx, the rounding order of dense()
+            torch.mul((gz[z][None, :] * gy)[:, None, :], gx[None, :, :], out=view[z, ..., 0])
+            view[z, ..., 0].neg_()
+        return out
 
 
 def _axes(interior, pml):
@@ -191,6 +256,67 @@ def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, pp
                          omega=omega, sources=centres, layer_tops=tops.tolist()))
 
 
+def large_layered(interior=(200, 200, 100), pml=10, k=64, seed=1005, n_layers=12, ppw=10.0, n_faults=3):
+    """Large case: 12 layers of 1.5-6.0 (km/s) whose interface depths jitter
+    by +-15 % of the layer thickness, offset across three dipping planar
+    faults and arched by one anticline (interfaces raised by a Gaussian
+    ridge about a seeded horizontal fold axis); spacing h = 1/(max interior
+    + 1) (km), omega for ``ppw`` points per wavelength in the slowest layer,
+    and k Gaussian point sources (width 2h) at seeded interior points at
+    least PML+2 points from every face.  The sources are kept separable, so
+    the (nz, ny, nx, k) array (6 GB at k = 64) is only built when asked for."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    n = [m + 2 * pml for m in interior]
+    h = 1.0 / (max(interior) + 1)
+    X, Y, Z = [(np.arange(nn) - pml + 1) * h for nn in n]
+    Zc, Yc, Xc = np.meshgrid(Z, Y, X, indexing="ij")
+    depth = Z[-1] - Z[0]
+    speeds = np.linspace(1.5, 6.0, n_layers)
+    thick = depth / n_layers
+    tops = np.array([Z[0] + thick * (i + rng.uniform(-0.15, 0.15)) for i in range(1, n_layers)])
+    shift = np.zeros_like(Zc)
+    faults = []
+    width = [X[-1] - X[0], Y[-1] - Y[0]]
+    for _ in range(n_faults):
+        normal = np.array([rng.uniform(-1, 1), rng.uniform(-1, 1), rng.uniform(0.3, 0.8)])
+        normal /= np.linalg.norm(normal)
+        point = np.array([X[0] + rng.uniform(0.25, 0.75) * width[0], Y[0] + rng.uniform(0.25, 0.75) * width[1],
+                          0.5 * depth + Z[0]])
+        throw = rng.uniform(0.5, 1.0) * 0.3 * thick
+        side = (Xc - point[0]) * normal[0] + (Yc - point[1]) * normal[1] + (Zc - point[2]) * normal[2] > 0
+        shift = shift + np.where(side, throw, 0.0)
+        faults.append((normal.tolist(), point.tolist(), float(throw)))
+    # anticline: interfaces raised by amp * exp(-d^2 / (2 w^2)), d the
+    # horizontal distance to the fold axis through `axis_point` at `azimuth`
+    azimuth = rng.uniform(0, math.pi)
+    axis_point = (X[0] + rng.uniform(0.3, 0.7) * width[0], Y[0] + rng.uniform(0.3, 0.7) * width[1])
+    fold_amp = rng.uniform(1.0, 2.0) * thick
+    fold_w = rng.uniform(0.1, 0.2) * max(width)
+    dist = -(Xc - axis_point[0]) * math.sin(azimuth) + (Yc - axis_point[1]) * math.cos(azimuth)
+    fold = fold_amp * np.exp(-dist ** 2 / (2 * fold_w ** 2))
+    del dist
+    # z index 0 is the top face (sweep coordinate v = nz-1-z): depth grows
+    # with z and the slow layer sits at the surface
+    layer = np.searchsorted(tops, Zc - shift + fold)
+    vel = np.ascontiguousarray(speeds[np.clip(layer, 0, n_layers - 1)])
+    del Xc, Yc, Zc, shift, fold, layer
+    omega = 2 * math.pi * speeds[0] / (ppw * h)
+    w = [(nn + 1) * h for nn in n]
+    disc = Discretization(omega, n[0], n[1], n[2], w[0], w[1], w[2], bcs=(PML,) * 5, pml=(pml,) * 3, sigma=SIGMA)
+    sig = 2.0 * h
+    g = [np.zeros((k, nn)) for nn in n]
+    centres = []
+    for r in range(k):
+        idx = [int(rng.integers(pml + 2, nn - pml - 2)) for nn in n]
+        centres.append(idx)
+        for a, (ax, i) in enumerate(zip((X, Y, Z), idx)):
+            g[a][r] = np.exp(-((ax - ax[i]) ** 2) / (2 * sig ** 2))
+    return Workload("large_layered", disc, vel, SeparableSources(*g), pml, interior,
+                    dict(h=h, omega=omega, sources=centres, layer_tops=tops.tolist(), faults=faults,
+                         anticline=dict(azimuth=azimuth, axis_point=list(axis_point), amplitude=fold_amp,
+                                        width=fold_w)))
+
+
 def batch_problems(count=48, seed=1003, sides=tuple(range(32, 97, 4)), pml=5, ppw_range=(8.0, 12.0),
                    k_range=(1, 8), n_anom=3):
     """Batching case: ``count`` independent problems, every side drawn from
@@ -234,4 +360,8 @@ CONFIGS = {
     "layered_faults_96": layered_faults,
     # test-sized member of the same family
     "layered_faults_24": lambda: layered_faults(interior=(20, 20, 16), pml=5, k=4, ppw=12.0),
+    # the large configuration: 200 x 200 x 100 interior + 10 PML points per face
+    "large_220": large_layered,
+    # a small member of the large family (same generator, same ppw and PML)
+    "large_60": lambda: large_layered(interior=(40, 40, 20), pml=10, k=16),
 }

@@ -34,6 +34,26 @@ def test_noalloc_multiply_matches_allocating_multiply(product_lib):
         assert rel(got.cpu().numpy(), ref.cpu().numpy()) < 1e-13, call
 
 
+def test_noalloc_multiply_leaves_device_memory_untouched(product_lib):
+    """After the first call on a device (which only resolves the array's
+    address), repeated calls change neither the device's free memory nor
+    the caller's current device."""
+    import torch
+    w = W.small_case(interior=(12, 13, 14), pml=5, freq=2.0, k=2, seed=21)
+    H = P.DistHelmholtz(w.disc)
+    H.Initialize(w.velocity, precision=P.FP64)
+    B = torch.from_numpy(w.rhs.reshape(-1).copy()).cuda()
+    H.multiply_device_noalloc(B)
+    torch.cuda.synchronize()
+    dev = torch.cuda.current_device()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        H.multiply_device_noalloc(B)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.current_device() == dev
+
+
 def test_noalloc_multiply_rejects_grids_beyond_its_scratch(product_lib):
     import torch
     w = W.small_case(interior=(12, 13, 14), pml=5, freq=2.0, k=1, seed=21)
