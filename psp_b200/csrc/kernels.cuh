@@ -223,15 +223,18 @@ void LaunchSweepBackward(const SweepFront<R>* fr, const SweepTile* tiles, int n,
                          const PanelIO& io, const SweepWork& w, cudaStream_t st);
 
 // Tensor-core (tcgen05, split TF32) forms for complex-single factors
-// (sweep_tc.cu); tiles of kTcRows rows, any K-chunk length.
+// (sweep_tc.cu); tiles of kTcRows rows, any K-chunk length, and `cols` (16
+// or 32) right-hand sides per tile: the tile list's col0 steps by `cols`,
+// and a split tile's partial slots and counters are per 16-column sub-tile
+// (slot (t.slot + split) * cols / 16 + h, counter t.counter * cols / 16 + h).
 void PrepareSweepTcKernels();
 // Bytes of the two TMA maps of one front, and their encoding (host) into
 // out (64-byte aligned host memory) for the front's G, s, u and ldg.
 constexpr size_t kSweepTcMapBytes = 256;
 void EncodeSweepTcMaps(const SweepFront<float>& f, void* out);
-void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, const SweepWork& w,
-                          cudaStream_t st);
-void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k,
+void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols,
+                          const SweepWork& w, cudaStream_t st);
+void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k, int cols,
                            const PanelIO& io, const SweepWork& w, cudaStream_t st);
 
 // ------------------------------------------------------------------ GMRES vectors

@@ -271,6 +271,7 @@ private:
     // and the K-chunk of its tiles.
     struct SweepVariant {
         bool tc = false;
+        int cols = kSweepCols;  // right-hand sides per tile (tensor cores: 16 or 32)
         int chunk = 0;
         size_t tiles = 0;  // arena offset of the tile list
         int n = 0;
@@ -909,16 +910,17 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // nothing extra and save split-K partial sums) and only shrinks to give
     // every SM tiles; `forceChunk` > 0 fixes it instead (tuning candidates).
     int64_t maxPartialRows = kTcRows, maxCounters = 1;
-    auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, bool tcTiles, int forceChunk,
+    auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, bool tcTiles, int cols, int forceChunk,
                          std::vector<SweepTile>& tiles) {
         const int maxChunk = tcTiles ? 512 : SweepMaxChunk<R>();
         const int tileRows = tcTiles ? kTcRows : kSweepRows;
+        const int subs = cols / kSweepCols;  // partial slots and counters per split tile
         auto build = [&](int kc, bool emit) {
             int64_t n = 0, slots = 0, counters = 0;
             for (int t : depthNodes_[d]) {
                 const int s = cs.size[t], u = cs.usize[t];
                 const int M = fwd ? s + u : s, K = fwd ? s : s + u;
-                for (int col0 = 0; col0 < k; col0 += kSweepCols)
+                for (int col0 = 0; col0 < k; col0 += cols)
                     for (int row0 = 0; row0 < M; row0 += tileRows) {
                         const int kb = fwd ? 0 : row0;
                         const int ke = fwd ? std::min(K, row0 + tileRows) : K;
@@ -940,8 +942,8 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
                     }
             }
             if (emit) {
-                maxPartialRows = std::max(maxPartialRows, slots * tileRows);
-                maxCounters = std::max(maxCounters, counters);
+                maxPartialRows = std::max(maxPartialRows, slots * tileRows * subs);
+                maxCounters = std::max(maxCounters, counters * subs);
             }
             return n;
         };
@@ -969,25 +971,32 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // Candidates of one depth and direction: the default tiling of each
     // kernel and, with tensor cores, the other chunk lengths (a tiling equal
     // to an earlier candidate's is skipped).
+    // With more than 16 right-hand sides the tensor-core tiles take 32 of
+    // them (one split of each G stage for twice the columns); the 16-wide
+    // default stays a candidate.
     auto makeVariants = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepVariant>& out) {
-        std::vector<std::pair<bool, int>> cand;
+        struct Cand { bool tc; int cols, chunk; };
+        std::vector<Cand> cand;
         if (tc_) {
-            cand.push_back({true, 0});
-            for (int kc : {64, 128, 256, 512}) cand.push_back({true, kc});
-            cand.push_back({false, 0});
-            for (int kc : {64, 128}) cand.push_back({false, kc});
+            const int wide = k > kSweepCols ? 32 : kSweepCols;
+            cand.push_back({true, wide, 0});
+            for (int kc : {64, 128, 256, 512}) cand.push_back({true, wide, kc});
+            if (wide != kSweepCols) cand.push_back({true, kSweepCols, 0});
+            cand.push_back({false, kSweepCols, 0});
+            for (int kc : {64, 128}) cand.push_back({false, kSweepCols, kc});
         } else {
-            cand.push_back({false, 0});
+            cand.push_back({false, kSweepCols, 0});
         }
         std::vector<std::vector<SweepTile>> seen;
         for (const auto& cd : cand) {
             std::vector<SweepTile> tiles;
             SweepVariant v;
-            v.tc = cd.first;
-            v.chunk = makeTiles(cs, d, fwd, cd.first, cd.second, tiles);
+            v.tc = cd.tc;
+            v.cols = cd.cols;
+            v.chunk = makeTiles(cs, d, fwd, cd.tc, cd.cols, cd.chunk, tiles);
             bool dup = false;
             for (size_t i = 0; i < seen.size() && !dup; ++i)
-                dup = out[i].tc == v.tc && seen[i].size() == tiles.size() &&
+                dup = out[i].tc == v.tc && out[i].cols == v.cols && seen[i].size() == tiles.size() &&
                       std::equal(tiles.begin(), tiles.end(), seen[i].begin(), [](const SweepTile& a, const SweepTile& b) {
                           return a.front == b.front && a.row0 == b.row0 && a.col0 == b.col0 && a.k0 == b.k0 &&
                                  a.k1 == b.k1;
@@ -1168,8 +1177,8 @@ bool FactorStore<R>::Autotune(SolvePlan& P) {
                         const std::vector<SweepVariant>& vs = (dir ? cp.bVar : cp.fVar)[d];
                         std::fprintf(stderr, dir ? "  bwd" : " fwd");
                         for (size_t i = 0; i < vs.size(); ++i)
-                            std::fprintf(stderr, " %s%s%d %.4f", (int)i == (dir ? cp.bSel : cp.fSel)[d] ? "*" : "",
-                                         vs[i].tc ? "tc" : "cc", vs[i].chunk, best[dir][d][i]);
+                            std::fprintf(stderr, " %s%s%d/%d %.4f", (int)i == (dir ? cp.bSel : cp.fSel)[d] ? "*" : "",
+                                         vs[i].tc ? "tc" : "cc", vs[i].cols, vs[i].chunk, best[dir][d][i]);
                     }
                     std::fprintf(stderr, "\n");
                 }
@@ -1224,7 +1233,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
         bool done = false;
         if constexpr (std::is_same<R, float>::value) {
             if (v.tc) {
-                LaunchSweepForwardTc(fr, tl, v.n, k, w, st);
+                LaunchSweepForwardTc(fr, tl, v.n, k, v.cols, w, st);
                 done = true;
             }
         }
@@ -1244,7 +1253,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
         bool done = false;
         if constexpr (std::is_same<R, float>::value) {
             if (v.tc) {
-                LaunchSweepBackwardTc(fr, tl, v.n, B, k, io, w, st);
+                LaunchSweepBackwardTc(fr, tl, v.n, B, k, v.cols, io, w, st);
                 done = true;
             }
         }

@@ -6,15 +6,17 @@
 // one real product on the tensor core: A's rows read as interleaved
 // (re, im) pairs form a rows x 2K real matrix, and every complex entry b of
 // B becomes the 2x2 real block [[re b, im b], [-im b, re b]] of a 2K x 32
-// real matrix, so the 32 real accumulator columns are C's interleaved
+// real matrix, so the 2 NC real accumulator columns are C's interleaved
 // (re, im) pairs.  Each operand is split into tf32 head and tail
 // (x = hi + lo) and hi*hi + hi*lo + lo*hi is accumulated in FP32 in tensor
 // memory (about FP32 accuracy from TF32 inputs) with two MMAs per 8-value K
-// step: A_hi [B_hi | B_lo] (N = 64) and A_lo B_hi (N = 32, onto the first 32
-// columns); the epilogue adds the two 32-column halves.
+// step: A_hi [B_hi | B_lo] (N = 4 NC) and A_lo B_hi (N = 2 NC, onto the first
+// 2 NC columns); the epilogue adds the two halves.
 //
-// A tile is 128 rows (one UMMA M=128 accumulator) x 16 right-hand sides over
-// one K-chunk, consumed in stages of 16 complex K-columns.  The kernels are
+// A tile is 128 rows (one UMMA M=128 accumulator) x NC right-hand sides
+// (NC = 16, or 32 when a launch has more than 16: every G stage is then split
+// once for twice the right-hand sides) over one K-chunk, consumed in stages
+// of 16 complex K-columns.  The kernels are
 // persistent (one CTA per SM walks the tiles blockIdx.x, blockIdx.x + grid,
 // ...) and warp-specialized, with mbarriers between the roles:
 //   producer (1 thread) one tiled TMA copy per stage of G's 128 x 16 box
@@ -59,62 +61,79 @@ constexpr int kGroupThreads = kLoadThreads / kGroups; // 128
 
 constexpr int kStageK = 16;                            // complex K per stage (one 128-byte swizzle row)
 constexpr uint32_t kAPlane = kTcRows * 128;            // 16 KB
-constexpr uint32_t kBPlane = 2 * kSweepCols * 128;     // 4 KB: 32 rows
-constexpr uint32_t kPlaneSet = 2 * kAPlane + 2 * kBPlane;  // A hi, A lo, B hi, B lo (B lo right after B hi)
 constexpr int kPlaneSets = kGroups;                    // one per converter group
-constexpr uint32_t kAccCols = 4 * kSweepCols;          // f32 columns per accumulator (two halves)
-constexpr int kAccs = 4;                               // accumulators (tiles in flight per CTA)
 // The forward kernel keeps each plane set's split A stage in TMEM after the
 // accumulators (head then tail, 2 kStageK columns each, lane = row): the MMA
 // reads A from tensor memory and only B's planes go through shared memory.
 constexpr uint32_t kAStageCols = 2 * kStageK;
-__host__ __device__ constexpr uint32_t ACol(int ps) { return kAccs * kAccCols + (uint32_t)ps * 2 * kAStageCols; }
 constexpr uint32_t kTmemCols = 512;
-static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
-constexpr uint32_t kIdescN64 = umma::InstrDescTf32(kTcRows, 4 * kSweepCols);
-constexpr uint32_t kIdescN32 = umma::InstrDescTf32(kTcRows, 2 * kSweepCols);
+constexpr uint32_t kRawA = kStageK * kTcRows * 8;      // 16 KB
+constexpr int kRawMax = 8;
+constexpr int kAccMax = 4, kOwnMax = 3;
 
-// The result tile passes through shared memory with row stride kOutPad.
+// The result passes through shared memory 16 right-hand sides (one sub-tile)
+// at a time, with row stride kOutPad.
 constexpr int kOutPad = kSweepCols + 1;
 constexpr uint32_t kStaging = kTcRows * kOutPad * 8;
 constexpr int kOutRowsPerPass = kEpiThreads / kSweepCols;  // 8
 constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 
-// Raw data of the stages in flight.
-//   A arrives by one tiled TMA copy per stage into a ring of RawSlots(fwd)
-//   slots shared by both groups: forward G's 128-row x 16-column box
-//   ([kc][row]), backward G^T's 128 x 16 box ([row][kc]).  The forward keeps
-//   A in TMEM, so its last four slots reuse the A planes of the plane sets.
-//   Each group: a ring of kOwn slots of its own copies of B (forward
-//   [plane][kc][n], backward [kc][n]), every entry read back by the thread
-//   that copied it.
-constexpr int kRawMax = 8;
-__host__ __device__ constexpr int RawSlots(bool fwd) { return fwd ? 8 : 6; }
-__host__ __device__ constexpr int RawInRegion(bool fwd) { return fwd ? 4 : 6; }
-constexpr int kAheadOwn = 2;                           // own stages in flight per group
-constexpr int kOwn = kAheadOwn + 1;
-constexpr uint32_t kRawA = kStageK * kTcRows * 8;      // 16 KB
-__host__ __device__ constexpr uint32_t OwnSlot(bool fwd) {
-    return fwd ? 3 * kStageK * kSweepCols * 8 : kStageK * kSweepCols * 8;
-}
-__host__ __device__ constexpr uint32_t OwnBase(bool fwd) { return RawInRegion(fwd) * kRawA; }
-constexpr uint32_t kRegionOff = kPlaneSets * kPlaneSet;
-static_assert(RawSlots(true) - RawInRegion(true) == 2 * kPlaneSets && kRawA == kAPlane,
-              "the forward's extra raw slots are the plane sets' A planes");
-constexpr uint32_t kRegion =
-    (OwnBase(true) + kGroups * kOwn * OwnSlot(true)) > (OwnBase(false) + kGroups * kOwn * OwnSlot(false))
-        ? (OwnBase(true) + kGroups * kOwn * OwnSlot(true))
-        : (OwnBase(false) + kGroups * kOwn * OwnSlot(false));
-constexpr uint32_t kStagingOff = kRegionOff + kRegion;
-constexpr size_t kTcSmem = kStagingOff + kStaging + 1024;
-static_assert(kTcSmem <= 232448, "shared memory per CTA");
+// Shapes of the kernels with NC right-hand sides per tile.
+//   B planes: 2 NC rows of B' (hi, then lo right after it).
+//   Accumulators: 4 NC f32 columns each ([A_hi B_hi + A_lo B_hi | A_hi B_lo]),
+//   kAccs of them (tiles in flight per CTA).
+//   Raw data of the stages in flight: A arrives by one tiled TMA copy per
+//   stage into a ring of RawSlots(fwd) slots shared by both groups (forward
+//   G's 128-row x 16-column box, [kc][row]; backward G^T's 128 x 16 box,
+//   [row][kc]); the forward keeps A in TMEM, so its last four slots reuse
+//   the A planes of the plane sets.  Each group has a ring of kOwn slots of
+//   its own copies of B (forward [plane][kc][n], backward [kc][n]), every
+//   entry read back by the thread that copied it.
+template <int NC>
+struct Cfg {
+    static constexpr int kCols = NC;
+    static constexpr int kSubs = NC / kSweepCols;                    // 16-column sub-tiles
+    static constexpr uint32_t kBPlane = 2 * NC * 128;
+    static constexpr uint32_t kPlaneSet = 2 * kAPlane + 2 * kBPlane;  // A hi, A lo, B hi, B lo
+    static constexpr uint32_t kAccCols = 4 * NC;
+    static constexpr int kAccs = NC == 16 ? 4 : 2;
+    static constexpr uint32_t kIdescHi = umma::InstrDescTf32(kTcRows, 4 * NC);
+    static constexpr uint32_t kIdescLo = umma::InstrDescTf32(kTcRows, 2 * NC);
+    static constexpr int kAheadOwn = NC == 16 ? 2 : 1;              // own stages in flight per group
+    static constexpr int kOwn = kAheadOwn + 1;
+    __host__ __device__ static constexpr int RawSlots(bool fwd) { return NC == 16 ? (fwd ? 8 : 6) : (fwd ? 7 : 5); }
+    __host__ __device__ static constexpr int RawInRegion(bool fwd) {
+        return NC == 16 ? (fwd ? 4 : 6) : (fwd ? 3 : 5);
+    }
+    __host__ __device__ static constexpr uint32_t OwnSlot(bool fwd) {
+        return fwd ? 3 * kStageK * NC * 8 : kStageK * NC * 8;
+    }
+    __host__ __device__ static constexpr uint32_t OwnBase(bool fwd) { return RawInRegion(fwd) * kRawA; }
+    __host__ __device__ static constexpr uint32_t RegionBytes(bool fwd) {
+        return OwnBase(fwd) + kGroups * kOwn * OwnSlot(fwd);
+    }
+    static constexpr uint32_t kRegionOff = kPlaneSets * kPlaneSet;
+    static constexpr uint32_t kRegion = RegionBytes(true) > RegionBytes(false) ? RegionBytes(true) : RegionBytes(false);
+    static constexpr uint32_t kStagingOff = kRegionOff + kRegion;
+    static constexpr size_t kSmem = kStagingOff + kStaging + 1024;
+    __host__ __device__ static constexpr uint32_t ACol(int ps) {
+        return kAccs * kAccCols + (uint32_t)ps * 2 * kAStageCols;
+    }
+    static_assert(RawSlots(true) - RawInRegion(true) == 2 * kPlaneSets && kRawA == kAPlane,
+                  "the forward's extra raw slots are the plane sets' A planes");
+    static_assert(RawSlots(true) <= kRawMax && RawSlots(false) <= kRawMax, "raw ring");
+    static_assert(kAccs <= kAccMax && kOwn <= kOwnMax, "sync arrays");
+    static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
+    static_assert(kSmem <= 232448, "shared memory per CTA");
+};
 
 // Raw A slot `slot` (shared-memory base `smem`, 1 KB aligned).
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ __forceinline__ unsigned char* RawSlotPtr(unsigned char* smem, int slot) {
-    if (slot < RawInRegion(kFwd)) return smem + kRegionOff + slot * kRawA;
-    const int e = slot - RawInRegion(kFwd);
-    return smem + (e / 2) * kPlaneSet + (e % 2) * kAPlane;
+    using C = Cfg<NC>;
+    if (slot < C::RawInRegion(kFwd)) return smem + C::kRegionOff + slot * kRawA;
+    const int e = slot - C::RawInRegion(kFwd);
+    return smem + (e / 2) * C::kPlaneSet + (e % 2) * kAPlane;
 }
 
 // Stage description handed from the loaders to the MMA thread.
@@ -124,10 +143,10 @@ struct StageHdr {
 
 struct Sync {
     uint64_t planeFull[kPlaneSets], planeEmpty[kPlaneSets];
-    uint64_t accFull[kAccs], accEmpty[kAccs];
+    uint64_t accFull[kAccMax], accEmpty[kAccMax];
     uint64_t rawFull[kRawMax], rawEmpty[kRawMax];
     StageHdr hdr[kPlaneSets];
-    int ownInfo[kGroups][kOwn];  // stage place, packed (see InfoSt); written and read by a group's first thread
+    int ownInfo[kGroups][kOwnMax];  // stage place, packed (see InfoSt); written and read by a group's first thread
     int rawK[kRawMax][2];        // stage's first K index and the tile's K end
     uint32_t tmem;
     int abort;
@@ -278,15 +297,16 @@ struct LoadCursor {
 // kBase), backward the 16 x 128 box of G at (kBase, row0), i.e. 128 rows of
 // G^T.  Rows or columns outside G arrive as zeros; K columns past the tile's
 // range are masked by the converters.
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
                              int k, unsigned char* smem, Sync& S, int* status) {
+    using C = Cfg<NC>;
     if ((threadIdx.x & 31) != 0) return;
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
     for (int g = 0; cur.Valid(g); ++g) {
-        const int slot = g % RawSlots(kFwd);
-        if (g >= RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / RawSlots(kFwd)) - 1) & 1, S, status)) return;
+        const int slot = g % C::RawSlots(kFwd);
+        if (g >= C::RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / C::RawSlots(kFwd)) - 1) & 1, S, status)) return;
         const LoadMeta& m = cur.m;
         const int kBase = cur.KBase();
         S.rawK[slot][0] = kBase;
@@ -294,9 +314,9 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
         umma::MbarArriveExpectTx(&S.rawFull[slot], kRawA);
         const unsigned char* map = reinterpret_cast<const unsigned char*>(m.tmap) + (kFwd ? 0 : 128);
         if (kFwd)
-            umma::TmaLoad2D(RawSlotPtr<kFwd>(smem, slot), map, m.row0, kBase, &S.rawFull[slot]);
+            umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, m.row0, kBase, &S.rawFull[slot]);
         else
-            umma::TmaLoad2D(RawSlotPtr<kFwd>(smem, slot), map, kBase, m.row0, &S.rawFull[slot]);
+            umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, kBase, m.row0, &S.rawFull[slot]);
         cur.Advance();
     }
 }
@@ -313,31 +333,32 @@ __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
 // B entries; backward also its eight 16-byte A chunks, zero-filled outside
 // the tile), commits one copy group and moves the cursor to the group's
 // next stage.
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* own, int gr, Sync& S) {
+    using C = Cfg<NC>;
     if (cur.total >= 0) {
         umma::CpAsyncCommit();
         return;
     }
-    const int slot = (cur.gl / kGroups) % kOwn;
+    const int slot = (cur.gl / kGroups) % C::kOwn;
     const LoadMeta& m = cur.m;
     const int ct = (threadIdx.x - kLoad0) % kGroupThreads;
     if (ct == 0) S.ownInfo[gr][slot] = cur.Info();
-    unsigned char* base = own + slot * OwnSlot(kFwd);
+    unsigned char* base = own + slot * C::OwnSlot(kFwd);
     c32* rb = reinterpret_cast<c32*>(base);
-    const int ncol = min(kSweepCols, cur.k - m.col0);
+    const int ncol = min(NC, cur.k - m.col0);
     const int kBase = cur.KBase();
 #pragma unroll
-    for (int j = 0; j < kStageK * kSweepCols / kGroupThreads; ++j) {
+    for (int j = 0; j < kStageK * NC / kGroupThreads; ++j) {
         const int e = ct + j * kGroupThreads;
-        const int kc = e / kSweepCols, nn = e % kSweepCols;
+        const int kc = e / NC, nn = e % NC;
         const int kk = kBase + kc;
         const bool ok = kk < m.ke && nn < ncol;
         if (kFwd) {
             const c32* src = m.B + (int64_t)kk * 3 * cur.k + m.col0 + nn;
 #pragma unroll
             for (int p = 0; p < 3; ++p)
-                umma::CpAsync8(rb + p * kStageK * kSweepCols + e, ok ? src + p * cur.k : m.B, ok ? 8u : 0u);
+                umma::CpAsync8(rb + p * kStageK * NC + e, ok ? src + p * cur.k : m.B, ok ? 8u : 0u);
         } else {
             umma::CpAsync8(rb + e, ok ? m.B + (int64_t)kk * cur.k + m.col0 + nn : m.B, ok ? 8u : 0u);
         }
@@ -349,9 +370,10 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
 
 // Converts one raw stage into plane set P (thread ct of a group); forward
 // K-columns at or beyond kValid are taken as zero.
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawA, const unsigned char* own,
                                              int kValid, int ct, uint32_t tmemA) {
+    using C = Cfg<NC>;
     unsigned char* aHi = P;
     unsigned char* aLo = P + kAPlane;
     const c32 zero = mk<float>(0, 0);
@@ -390,12 +412,12 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
     // B: entry (kc, n) becomes rows 2n, 2n+1 of B' at K positions 2kc, 2kc+1
     const c32* rb = reinterpret_cast<const c32*>(own);
     unsigned char* bHi = P + 2 * kAPlane;
-    unsigned char* bLo = bHi + kBPlane;
+    unsigned char* bLo = bHi + C::kBPlane;
 #pragma unroll
-    for (int j = 0; j < kStageK * kSweepCols / kGroupThreads; ++j) {
+    for (int j = 0; j < kStageK * NC / kGroupThreads; ++j) {
         const int e = ct + j * kGroupThreads;
-        const int kc = e / kSweepCols, nn = e % kSweepCols;
-        const c32 b = kFwd ? rb[e] + rb[kStageK * kSweepCols + e] + rb[2 * kStageK * kSweepCols + e] : rb[e];
+        const int kc = e / NC, nn = e % NC;
+        const c32 b = kFwd ? rb[e] + rb[kStageK * NC + e] + rb[2 * kStageK * NC + e] : rb[e];
         float2 h, l;
         Split2(b, h, l);
         const uint32_t o0 = umma::Sw128Offset(2 * nn, kc >> 1) + (kc & 1) * 8;
@@ -409,18 +431,19 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
 
 // Converts stage g (a stage of this thread's group, plane set g % 2) or
 // ends the stream; false when the role is done.
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char* own, const LoadCursor<kFwd>& cur,
                                               int g, int gr, int ct, Sync& S, int* status) {
-    const int ps = gr, slot = g % RawSlots(kFwd), oslot = (g / kGroups) % kOwn;
+    using C = Cfg<NC>;
+    const int ps = gr, slot = g % C::RawSlots(kFwd), oslot = (g / kGroups) % C::kOwn;
     const bool valid = cur.Valid(g);
-    if (valid && !Wait(&S.rawFull[slot], (g / RawSlots(kFwd)) & 1, S, status)) return false;
+    if (valid && !Wait(&S.rawFull[slot], (g / C::RawSlots(kFwd)) & 1, S, status)) return false;
     if (g >= kGroups && !Wait(&S.planeEmpty[ps], ((g / kGroups) - 1) & 1, S, status)) return false;
-    umma::CpAsyncWait<kAheadOwn>();  // this thread's own copies of stage g have landed
+    umma::CpAsyncWait<C::kAheadOwn>();  // this thread's own copies of stage g have landed
     if (valid) {
         const int kValid = S.rawK[slot][1] - S.rawK[slot][0];
-        ConvertStage<kFwd>(smem + ps * kPlaneSet, RawSlotPtr<kFwd>(smem, slot), own + oslot * OwnSlot(kFwd),
-                           kValid, ct, S.tmem + ACol(ps));
+        ConvertStage<NC, kFwd>(smem + ps * C::kPlaneSet, RawSlotPtr<NC, kFwd>(smem, slot),
+                               own + oslot * C::OwnSlot(kFwd), kValid, ct, S.tmem + C::ACol(ps));
     }
     if (kFwd) {
         umma::TmemStoreWait();
@@ -436,58 +459,61 @@ __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char
     return valid;
 }
 
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
                               int k, unsigned char* smem, Sync& S, int* status) {
+    using C = Cfg<NC>;
     const int lt = threadIdx.x - kLoad0;
     const int gr = lt / kGroupThreads, ct = lt % kGroupThreads;
-    unsigned char* own = smem + kRegionOff + OwnBase(kFwd) + gr * kOwn * OwnSlot(kFwd);
+    unsigned char* own = smem + C::kRegionOff + C::OwnBase(kFwd) + gr * C::kOwn * C::OwnSlot(kFwd);
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
     for (int i = 0; i < gr; ++i) cur.Advance();
     PdlWait();  // right-hand sides come from the preceding kernels
 #pragma unroll
-    for (int a = 0; a < kAheadOwn; ++a) IssueOwn(cur, own, gr, S);
+    for (int a = 0; a < C::kAheadOwn; ++a) IssueOwn<NC>(cur, own, gr, S);
     for (int g = gr;; g += kGroups) {
-        IssueOwn(cur, own, gr, S);
-        if (!ConverterStep<kFwd>(smem, own, cur, g, gr, ct, S, status)) break;
+        IssueOwn<NC>(cur, own, gr, S);
+        if (!ConverterStep<NC, kFwd>(smem, own, cur, g, gr, ct, S, status)) break;
     }
     umma::CpAsyncWaitAll();
 }
 
 // ------------------------------------------------------------------ MMA
 
-// `init`: the accumulator starts from its current contents (the forward
-// epilogue preloads it); otherwise the tile's first MMA overwrites it.
+// `init`: accumulate onto the accumulator's contents (every stage of a tile
+// but its first); otherwise the MMA overwrites it.
 // Forward: A's split stage is read from TMEM at tmemA (head, then tail).
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ __forceinline__ void IssueStage(const unsigned char* P, uint32_t tmem, uint32_t tmemA, bool init) {
+    using C = Cfg<NC>;
     const uint32_t aHi = umma::SmemAddr(P), aLo = aHi + kAPlane, bHi = aHi + 2 * kAPlane;
 #pragma unroll
     for (int s = 0; s < 2 * kStageK / 8; ++s) {
         const uint32_t o = s * 32;
         const uint64_t bd = umma::SmemDescSw128(bHi + o);
         if (kFwd) {
-            umma::MmaTf32TmemA(tmem, tmemA + 8 * s, bd, kIdescN64, (init || s > 0) ? 1u : 0u);
-            umma::MmaTf32TmemA(tmem, tmemA + kAStageCols + 8 * s, bd, kIdescN32, 1u);
+            umma::MmaTf32TmemA(tmem, tmemA + 8 * s, bd, C::kIdescHi, (init || s > 0) ? 1u : 0u);
+            umma::MmaTf32TmemA(tmem, tmemA + kAStageCols + 8 * s, bd, C::kIdescLo, 1u);
         } else {
-            umma::MmaTf32(tmem, umma::SmemDescSw128(aHi + o), bd, kIdescN64, (init || s > 0) ? 1u : 0u);
-            umma::MmaTf32(tmem, umma::SmemDescSw128(aLo + o), bd, kIdescN32, 1u);
+            umma::MmaTf32(tmem, umma::SmemDescSw128(aHi + o), bd, C::kIdescHi, (init || s > 0) ? 1u : 0u);
+            umma::MmaTf32(tmem, umma::SmemDescSw128(aLo + o), bd, C::kIdescLo, 1u);
         }
     }
 }
 
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ void MmaRole(const unsigned char* planes, Sync& S, int* status) {
+    using C = Cfg<NC>;
     for (int g = 0;; ++g) {
         const int ps = g % kPlaneSets;
         if (!Wait(&S.planeFull[ps], (g / kPlaneSets) & 1, S, status)) return;
         const StageHdr h = S.hdr[ps];
         if (!h.valid) return;  // the epilogue counts its own tiles
-        const int b = h.j % kAccs;
-        if (h.st == 0 && !Wait(&S.accEmpty[b], (h.j / kAccs) & 1, S, status)) return;
+        const int b = h.j % C::kAccs;
+        if (h.st == 0 && !Wait(&S.accEmpty[b], (h.j / C::kAccs) & 1, S, status)) return;
         umma::FenceAfterSync();
-        IssueStage<kFwd>(planes + ps * kPlaneSet, S.tmem + b * kAccCols, S.tmem + ACol(ps), kFwd || h.st > 0);
+        IssueStage<NC, kFwd>(planes + ps * C::kPlaneSet, S.tmem + b * C::kAccCols, S.tmem + C::ACol(ps), h.st > 0);
         umma::CommitTo(&S.planeEmpty[ps]);
         if (h.st == h.nst - 1) umma::CommitTo(&S.accFull[b]);
     }
@@ -498,16 +524,17 @@ __device__ void MmaRole(const unsigned char* planes, Sync& S, int* status) {
 // Split-K over CTAs: partial tiles [slot][column][row]; the last CTA to arrive
 // sums them in split order.  Epilogue threads only (named barrier 1).
 __device__ __forceinline__ bool ReduceSplitsTc(const SweepTile& t, const SweepWork& w, Sync& S,
-                                               c32 (&acc)[kSweepCols]) {
+                                               c32 (&acc)[kSweepCols], int subs, int h) {
     if (t.nsplit <= 1) return true;
     c32* part = reinterpret_cast<c32*>(w.partials);
     const int row = threadIdx.x;
-    c32* mine = part + ((int64_t)(t.slot + t.split) * kSweepCols) * kTcRows;
+    const int counter = t.counter * subs + h;
+    c32* mine = part + ((int64_t)((t.slot + t.split) * subs + h) * kSweepCols) * kTcRows;
 #pragma unroll
     for (int n = 0; n < kSweepCols; ++n) mine[n * kTcRows + row] = acc[n];
     __threadfence();
     umma::NamedBarrier(1, kEpiThreads);
-    if (row == 0) S.isLast = (atomicAdd(w.counters + t.counter, 1) == t.nsplit - 1);
+    if (row == 0) S.isLast = (atomicAdd(w.counters + counter, 1) == t.nsplit - 1);
     umma::NamedBarrier(1, kEpiThreads);
     const bool last = S.isLast;
     umma::NamedBarrier(1, kEpiThreads);  // isLast is rewritten by the next tile
@@ -516,156 +543,166 @@ __device__ __forceinline__ bool ReduceSplitsTc(const SweepTile& t, const SweepWo
 #pragma unroll
     for (int n = 0; n < kSweepCols; ++n) acc[n] = mk<float>(0, 0);
     for (int s = 0; s < t.nsplit; ++s) {
-        const c32* p = part + ((int64_t)(t.slot + s) * kSweepCols) * kTcRows;
+        const c32* p = part + ((int64_t)((t.slot + s) * subs + h) * kSweepCols) * kTcRows;
 #pragma unroll
         for (int n = 0; n < kSweepCols; ++n) acc[n] += p[n * kTcRows + row];
     }
-    if (row == 0) w.counters[t.counter] = 0;
+    if (row == 0) w.counters[counter] = 0;
     return true;
 }
 
-// The epilogue keeps kAccs tiles in flight: while tile j's result is
-// written out, the accumulator it used is set up for tile j + kAccs (the
-// forward product starts from the update rows' own right-hand sides, which
-// are carried to the parent; every other entry starts at zero).  Thread e of
-// the epilogue handles column e % 16 of rows e / 16 + 8 i for global
-// accesses and TMEM lane (row) e for tensor memory; the two meet in the
-// shared-memory staging tile.
+// The epilogue drains one accumulator per tile while the MMAs of the next
+// kAccs - 1 tiles run: it loads the accumulator (lane = row), releases it at
+// once (the tile's first MMA overwrites it), and writes the result through a
+// shared-memory staging tile so that its global accesses are coalesced:
+// thread e handles column e % 16 of rows e / 16 + 8 i there.  A tile of NC
+// right-hand sides is written as NC / 16 sub-tiles of 16 (columns coff ..
+// coff + 15).  What a sub-tile's write-out reads from global memory (the
+// forward's carried right-hand sides of the update rows, which are added to
+// the product on the way to the parent; each row's parent row or natural
+// index) is loaded before its accumulator is ready.
 
 __device__ __forceinline__ bool TileOf(const SweepTile* tiles, int n, int j, int& ti) {
     ti = blockIdx.x + j * gridDim.x;
     return ti < n;
 }
 
-// Loads (coalesced) the forward carry of tile ti: sum of the three
-// right-hand-side planes of the update rows, split 0 only.
-__device__ __forceinline__ void LoadCarry(const SweepFront<float>* fr, const SweepTile* tiles, int ti, int k,
-                                          c32 (&carry)[kOutPerThread]) {
-    const SweepTile t = tiles[ti];
-    const SweepFront<float> f = fr[t.front];
+__device__ __forceinline__ int LdgIntIf(const int* p, bool pred) {
+    int x;
+    asm volatile(
+        "{\n\t.reg .pred q;\n\t"
+        "setp.ne.b32 q, %2, 0;\n\t"
+        "mov.b32 %0, -1;\n\t"
+        "@q ld.global.nc.b32 %0, [%1];\n\t}\n"
+        : "=r"(x)
+        : "l"(p), "r"((int)pred));
+    return x;
+}
+
+struct SubPrefetch {
+    c32 carry[kOutPerThread];  // forward: right-hand side of update row (sum of its three planes)
+    int idx[kOutPerThread];    // forward: the update row's row in the parent; backward: natural index
+};
+
+template <bool kFwd>
+__device__ __forceinline__ void PrefetchSub(const SweepFront<float>& f, const SweepTile& t, int k, int coff,
+                                            const PanelIO& io, SubPrefetch& pf) {
     const int e = threadIdx.x, n = e % kSweepCols;
-    const bool on = t.split == 0 && f.parentRb && t.col0 + n < k;
+    const int col = t.col0 + coff + n;
 #pragma unroll
     for (int i = 0; i < kOutPerThread; ++i) {
         const int r = t.row0 + e / kSweepCols + i * kOutRowsPerPass;
-        const bool ok = on && r >= f.s && r < f.s + f.u;
-        const c32* src = f.Rb + (int64_t)r * 3 * k + t.col0 + n;
-        carry[i] = LdgC32If(src, ok) + LdgC32If(src + k, ok) + LdgC32If(src + 2 * k, ok);
+        if (kFwd) {
+            const bool upd = r >= f.s && r < f.s + f.u;
+            pf.idx[i] = LdgIntIf(f.rel + (upd ? r - f.s : 0), upd);
+            const bool ok = upd && f.parentRb && col < k;
+            const c32* src = f.Rb + (int64_t)r * 3 * k + col;
+            pf.carry[i] = LdgC32If(src, ok) + LdgC32If(src + k, ok) + LdgC32If(src + 2 * k, ok);
+        } else {
+            const bool in = r < f.s;
+            pf.idx[i] = LdgIntIf(io.ndToNat + f.ndOff + (in ? r : 0), in);
+        }
     }
 }
 
-// Writes the carry into accumulator b (first 32 columns; the other half zero).
-__device__ __forceinline__ void InitAccumulator(Sync& S, int b, const c32 (&carry)[kOutPerThread], c32* staging) {
-    const int e = threadIdx.x, n = e % kSweepCols, warp = e / 32;
+// Sub-tile h of accumulator b (TMEM address taddr of this warp's lanes):
+// its columns of the first half plus the same columns of the second half.
+template <int NC>
+__device__ __forceinline__ void LoadAccumulator(uint32_t taddr, int h, c32 (&acc)[kSweepCols]) {
+    float v[kSweepCols];
 #pragma unroll
-    for (int i = 0; i < kOutPerThread; ++i) staging[(e / kSweepCols + i * kOutRowsPerPass) * kOutPad + n] = carry[i];
-    umma::NamedBarrier(1, kEpiThreads);
-    float v[2 * kSweepCols];
+    for (int q = 0; q < 2; ++q) {
+        umma::TmemLoad16(taddr + 2 * kSweepCols * h + kSweepCols * q, v);
 #pragma unroll
-    for (int c = 0; c < kSweepCols; ++c) {
-        const c32 x = staging[e * kOutPad + c];
-        v[2 * c] = x.re;
-        v[2 * c + 1] = x.im;
+        for (int c = 0; c < kSweepCols / 2; ++c) acc[8 * q + c] = mk(v[2 * c], v[2 * c + 1]);
     }
-    const uint32_t taddr = S.tmem + b * kAccCols + ((uint32_t)(warp * 32) << 16);
-    umma::TmemStore32(taddr, v);
 #pragma unroll
-    for (int c = 0; c < 2 * kSweepCols; ++c) v[c] = 0.f;
-    umma::TmemStore32(taddr + 2 * kSweepCols, v);
-    umma::NamedBarrier(1, kEpiThreads);  // staging is reused
+    for (int q = 0; q < 2; ++q) {
+        umma::TmemLoad16(taddr + 2 * NC + 2 * kSweepCols * h + kSweepCols * q, v);
+#pragma unroll
+        for (int c = 0; c < kSweepCols / 2; ++c) acc[8 * q + c] += mk(v[2 * c], v[2 * c + 1]);
+    }
 }
 
-// Coalesced write-out of a result tile from the staging tile.
+// Coalesced write-out of a sub-tile from the staging tile.
 template <bool kFwd>
-__device__ __forceinline__ void StoreTile(const SweepFront<float>& f, const SweepTile& t, int k, const c32* stage,
-                                          z64* B, c32* X, const PanelIO& io) {
+__device__ __forceinline__ void StoreTile(const SweepFront<float>& f, const SweepTile& t, int k, int coff,
+                                          const c32* stage, const SubPrefetch& pf, z64* B, c32* X,
+                                          const PanelIO& io) {
     const int e = threadIdx.x, n = e % kSweepCols;
-    if (t.col0 + n >= k) return;
+    const int col = t.col0 + coff + n;
+    if (col >= k) return;
     const int rows = kFwd ? f.s + f.u : f.s;
-#pragma unroll 4
+#pragma unroll
     for (int i = 0; i < kOutPerThread; ++i) {
         const int row = e / kSweepCols + i * kOutRowsPerPass;
         const int r = t.row0 + row;
-        if (r >= rows) break;
+        if (r >= rows) continue;
         const c32 v = stage[row * kOutPad + n];
         if (kFwd) {
-            if (r < f.s) f.Y[(int64_t)r * k + t.col0 + n] = v;
-            else if (f.parentRb) f.parentRb[((int64_t)f.rel[r - f.s] * 3 + 1 + f.childSlot) * k + t.col0 + n] = v;
+            if (r < f.s) f.Y[(int64_t)r * k + col] = v;
+            else if (f.parentRb) f.parentRb[((int64_t)pf.idx[i] * 3 + 1 + f.childSlot) * k + col] = v + pf.carry[i];
         } else {
-            X[(int64_t)(f.ndOff + r) * k + t.col0 + n] = v;
-            const int pn = io.ndToNat[f.ndOff + r];
+            X[(int64_t)(f.ndOff + r) * k + col] = v;
+            const int pn = pf.idx[i];
             const int xy = pn % io.nxy, vl = pn / io.nxy;
             if (vl < io.padding) continue;
-            z64* dst = B + (xy + (int64_t)(io.nz - 1 - (io.vOffset + vl)) * io.nxy) * io.ldk + t.col0 + n;
+            z64* dst = B + (xy + (int64_t)(io.nz - 1 - (io.vOffset + vl)) * io.nxy) * io.ldk + col;
             const z64 val = ccast<double>(v);
             *dst = io.outAccumulate ? *dst + val : val;
         }
     }
 }
 
-template <bool kFwd>
+template <int NC, bool kFwd>
 __device__ void EpilogueRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
                              int k, const SweepWork& w, c32* staging, Sync& S, z64* B, const PanelIO& io) {
+    using C = Cfg<NC>;
     const int warp = threadIdx.x / 32, row = threadIdx.x;
     c32* X = reinterpret_cast<c32*>(w.xnd);
     int ti;
     PdlWait();  // carries, split-K scratch and outputs are shared with the preceding kernels
-    // set up the first kAccs accumulators
-    for (int q = 0; q < kAccs && TileOf(tiles, n, q, ti); ++q) {
-        if (kFwd) {
-            c32 carry[kOutPerThread];
-            LoadCarry(fr, tiles, ti, k, carry);
-            InitAccumulator(S, q, carry, staging);
-            umma::FenceBeforeSync();
-        }
-        umma::MbarArrive(&S.accEmpty[q]);
-    }
+    for (int q = 0; q < C::kAccs; ++q) umma::MbarArrive(&S.accEmpty[q]);  // every accumulator starts free
     for (int j = 0; TileOf(tiles, n, j, ti); ++j) {
-        const int b = j % kAccs;
+        const int b = j % C::kAccs;
         const SweepTile t = tiles[ti];
         const SweepFront<float> f = fr[t.front];
-        int tn;
-        const bool more = TileOf(tiles, n, j + kAccs, tn);
-        c32 carry[kOutPerThread];
-        if (kFwd && more) LoadCarry(fr, tiles, tn, k, carry);
+        SubPrefetch pf;
+        PrefetchSub<kFwd>(f, t, k, 0, io, pf);
         // every epilogue thread takes the same branch (they share named barriers)
-        const bool ok = Wait(&S.accFull[b], (j / kAccs) & 1, S, w.status);
+        const bool ok = Wait(&S.accFull[b], (j / C::kAccs) & 1, S, w.status);
         if (umma::NamedBarrierOr(1, kEpiThreads, !ok)) return;
         umma::FenceAfterSync();
-        const uint32_t taddr = S.tmem + b * kAccCols + ((uint32_t)(warp * 32) << 16);
-        c32 acc[kSweepCols];
-        {
-            float v[2 * kSweepCols];
-            umma::TmemLoad32(taddr, v);
+        const uint32_t taddr = S.tmem + b * C::kAccCols + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
-            for (int c = 0; c < kSweepCols; ++c) acc[c] = mk(v[2 * c], v[2 * c + 1]);
-            umma::TmemLoad32(taddr + 2 * kSweepCols, v);
+        for (int h = 0; h < C::kSubs; ++h) {
+            if (h > 0) PrefetchSub<kFwd>(f, t, k, h * kSweepCols, io, pf);
+            c32 acc[kSweepCols];
+            LoadAccumulator<NC>(taddr, h, acc);
+            if (h == C::kSubs - 1) {
+                umma::FenceBeforeSync();
+                umma::MbarArrive(&S.accEmpty[b]);
+            }
+            if (!ReduceSplitsTc(t, w, S, acc, C::kSubs, h)) continue;
 #pragma unroll
-            for (int c = 0; c < kSweepCols; ++c) acc[c] += mk(v[2 * c], v[2 * c + 1]);
+            for (int c = 0; c < kSweepCols; ++c) staging[row * kOutPad + c] = acc[c];
+            umma::NamedBarrier(1, kEpiThreads);
+            StoreTile<kFwd>(f, t, k, h * kSweepCols, staging, pf, B, X, io);
+            umma::NamedBarrier(1, kEpiThreads);  // staging is rewritten next
         }
-        if (more) {
-            if (kFwd) InitAccumulator(S, b, carry, staging);
-            umma::FenceBeforeSync();
-            umma::MbarArrive(&S.accEmpty[b]);
-        }
-        if (!ReduceSplitsTc(t, w, S, acc)) continue;
-#pragma unroll
-        for (int c = 0; c < kSweepCols; ++c) staging[row * kOutPad + c] = acc[c];
-        umma::NamedBarrier(1, kEpiThreads);
-        StoreTile<kFwd>(f, t, k, staging, B, X, io);
-        umma::NamedBarrier(1, kEpiThreads);  // staging is rewritten by the next tile
     }
 }
 
 // ------------------------------------------------------------------ kernels
 
+template <int NC>
 __device__ __forceinline__ void InitSync(Sync& S) {
     if (threadIdx.x == 0) {
         for (int i = 0; i < kPlaneSets; ++i) {
             umma::MbarInit(&S.planeFull[i], kGroupThreads);
             umma::MbarInit(&S.planeEmpty[i], 1);
         }
-        for (int i = 0; i < kAccs; ++i) {
+        for (int i = 0; i < Cfg<NC>::kAccs; ++i) {
             umma::MbarInit(&S.accFull[i], 1);
             umma::MbarInit(&S.accEmpty[i], kEpiThreads);
         }
@@ -696,26 +733,29 @@ __device__ __forceinline__ unsigned char* SmemBase() {
     return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 }
 
+template <int NC>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const SweepFront<float>* __restrict__ fr,
                                                                          const SweepTile* __restrict__ tiles, int n,
                                                                          int k, SweepWork work) {
     __shared__ Sync S;
     unsigned char* smem = SmemBase();
     PdlTrigger();
-    InitSync(S);
+    InitSync<NC>(S);
     const int tid = threadIdx.x;
     if (tid < kLoad0) {
-        EpilogueRole<true>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + kStagingOff), S, nullptr, PanelIO{});
+        EpilogueRole<NC, true>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + Cfg<NC>::kStagingOff), S,
+                               nullptr, PanelIO{});
     } else if (tid < kMma0) {
-        ConverterRole<true>(fr, tiles, n, k, smem, S, work.status);
+        ConverterRole<NC, true>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
-        MmaRole<true>(smem, S, work.status);
+        MmaRole<NC, true>(smem, S, work.status);
     } else if (tid >= kProd0) {
-        ProducerRole<true>(fr, tiles, n, k, smem, S, work.status);
+        ProducerRole<NC, true>(fr, tiles, n, k, smem, S, work.status);
     }
     Teardown(S);
 }
 
+template <int NC>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const SweepFront<float>* __restrict__ fr,
                                                                           const SweepTile* __restrict__ tiles, int n,
                                                                           z64* __restrict__ B, int k, PanelIO io,
@@ -723,16 +763,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const 
     __shared__ Sync S;
     unsigned char* smem = SmemBase();
     PdlTrigger();
-    InitSync(S);
+    InitSync<NC>(S);
     const int tid = threadIdx.x;
     if (tid < kLoad0) {
-        EpilogueRole<false>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + kStagingOff), S, B, io);
+        EpilogueRole<NC, false>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + Cfg<NC>::kStagingOff), S, B,
+                                io);
     } else if (tid < kMma0) {
-        ConverterRole<false>(fr, tiles, n, k, smem, S, work.status);
+        ConverterRole<NC, false>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
-        MmaRole<false>(smem, S, work.status);
+        MmaRole<NC, false>(smem, S, work.status);
     } else if (tid >= kProd0) {
-        ProducerRole<false>(fr, tiles, n, k, smem, S, work.status);
+        ProducerRole<NC, false>(fr, tiles, n, k, smem, S, work.status);
     }
     Teardown(S);
 }
@@ -775,23 +816,37 @@ void PrepareSweepTcKernels() {
     int dev = 0;
     CUDA_CHECK(cudaGetDevice(&dev));
     CUDA_CHECK(cudaDeviceGetAttribute(&g_numSMs, cudaDevAttrMultiProcessorCount, dev));
-    CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kTcSmem));
-    CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kTcSmem));
+    CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_forward_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg<16>::kSmem));
+    CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_backward_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg<16>::kSmem));
+    CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_forward_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg<32>::kSmem));
+    CUDA_CHECK(cudaFuncSetAttribute(sweep_tc_backward_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Cfg<32>::kSmem));
 }
 
-void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, const SweepWork& w,
-                          cudaStream_t st) {
+void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols,
+                          const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    LaunchPdl(sweep_tc_forward_kernel, dim3(GridFor(n)), dim3(kTcThreads), kTcSmem, st, fr, tiles, n, k, w);
+    if (cols == 32)
+        LaunchPdl(sweep_tc_forward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles, n,
+                  k, w);
+    else
+        LaunchPdl(sweep_tc_forward_kernel<16>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<16>::kSmem, st, fr, tiles, n,
+                  k, w);
     CUDA_LAUNCH_CHECK();
 }
 
-void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k,
+void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k, int cols,
                            const PanelIO& io, const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    LaunchPdl(sweep_tc_backward_kernel, dim3(GridFor(n)), dim3(kTcThreads), kTcSmem, st, fr, tiles, n, B, k, io, w);
+    if (cols == 32)
+        LaunchPdl(sweep_tc_backward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles,
+                  n, B, k, io, w);
+    else
+        LaunchPdl(sweep_tc_backward_kernel<16>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<16>::kSmem, st, fr, tiles,
+                  n, B, k, io, w);
     CUDA_LAUNCH_CHECK();
 }
 

@@ -20,7 +20,14 @@ import numpy as np
 
 from . import PML, Discretization, DistUniformGrid
 
-SIGMA = 1.5  # UnitCube default --sigma (tests/UnitCube.cpp:28)
+SIGMA = 1.5  # UnitCube default --sigma (tests/UnitCube.cpp:28), for velocities near 1
+# PML amplitude of the velocity models in km/s: the reference's Overthrust
+# example (velocities of a few km/s) runs with --sigma 7.5
+# (doc/source/examples.rst:35; its default is 30, examples/Overthrust.cpp:33).
+# The stretch 1 + i (sigma/eta)(x/b)^2 (2 pi/omega) attenuates a wave of
+# speed c by exp(-2 pi sigma / (3 c)) across the layer, so the amplitude has
+# to grow with the velocities for the fast layers to be absorbed.
+SIGMA_KM = 7.5
 
 
 class Workload:
@@ -199,7 +206,8 @@ def small_case(interior=(12, 13, 14), pml=5, freq=2.0, k=3, seed=7, top_pml=True
                     dict(x0=x0.tolist(), sources=centres, freq=freq))
 
 
-def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, ppw=10.0, perturb=0.03):
+def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, ppw=10.0, perturb=0.03,
+                   sigma=SIGMA_KM):
     """Differentiation case: 8 layers of 1.5-5.5 (km/s) whose interface
     depths jitter by +-15 % of the layer thickness, offset across two dipping
     planar faults; uniform spacing h = 1/(max interior + 1) (km), and omega
@@ -233,7 +241,7 @@ def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, pp
     vel = np.ascontiguousarray(speeds[np.clip(layer, 0, n_layers - 1)])
     omega = 2 * math.pi * speeds[0] / (ppw * h)
     w = [(nn + 1) * h for nn in n]
-    disc = Discretization(omega, n[0], n[1], n[2], w[0], w[1], w[2], bcs=(PML,) * 5, pml=(pml,) * 3, sigma=SIGMA)
+    disc = Discretization(omega, n[0], n[1], n[2], w[0], w[1], w[2], bcs=(PML,) * 5, pml=(pml,) * 3, sigma=sigma)
     # sources and receivers on the first plane below the top PML (solver z index pml)
     zs = pml
     sig = 2.0 * h
@@ -256,7 +264,8 @@ def layered_faults(interior=(80, 80, 60), pml=8, k=32, seed=1004, n_layers=8, pp
                          omega=omega, sources=centres, layer_tops=tops.tolist()))
 
 
-def large_layered(interior=(200, 200, 100), pml=10, k=64, seed=1005, n_layers=12, ppw=10.0, n_faults=3):
+def large_layered(interior=(200, 200, 100), pml=10, k=64, seed=1005, n_layers=12, ppw=10.0, n_faults=3,
+                  sigma=SIGMA_KM):
     """Large case: 12 layers of 1.5-6.0 (km/s) whose interface depths jitter
     by +-15 % of the layer thickness, offset across three dipping planar
     faults and arched by one anticline (interfaces raised by a Gaussian
@@ -302,7 +311,7 @@ def large_layered(interior=(200, 200, 100), pml=10, k=64, seed=1005, n_layers=12
     del Xc, Yc, Zc, shift, fold, layer
     omega = 2 * math.pi * speeds[0] / (ppw * h)
     w = [(nn + 1) * h for nn in n]
-    disc = Discretization(omega, n[0], n[1], n[2], w[0], w[1], w[2], bcs=(PML,) * 5, pml=(pml,) * 3, sigma=SIGMA)
+    disc = Discretization(omega, n[0], n[1], n[2], w[0], w[1], w[2], bcs=(PML,) * 5, pml=(pml,) * 3, sigma=sigma)
     sig = 2.0 * h
     g = [np.zeros((k, nn)) for nn in n]
     centres = []

@@ -91,3 +91,28 @@ def test_mixed_route_solve_converges(setup):
         assert st["converged"] and st["final_max_rel_resid"] < 1e-6, name
         assert abs(st["iterations"] - sto["iterations"]) <= 2, name
         assert rel(Xm, X) < 1e-4, name
+
+
+def test_wide_tensor_core_tiles_match(product_lib):
+    """More than 16 right-hand sides: the tensor-core tiles take 32 (each G
+    stage split once for all of them; k = 40 leaves a partly filled last
+    tile, and the small fronts' short K-chunks exercise the split-K
+    reduction per 16-column sub-tile).  The preconditioner and every panel
+    solve agree with the CUDA-core kernels and the oracle, and a mixed
+    solve converges like the oracle's."""
+    w = W.small_case(**dict(CASE, k=40))
+    O = oracle_for(w.disc)
+    O.initialize(w.velocity)
+    wide = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": "0", "PSP_B200_SWEEP_CUDA_CORES": None})
+    cc = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": None, "PSP_B200_SWEEP_CUDA_CORES": "1"})
+    ref = O.precondition(w.rhs)
+    x = wide.precondition(w.rhs)
+    assert rel(x, ref) < 1e-4
+    assert rel(x, cc.precondition(w.rhs)) < 2e-5
+    for p in range(O.geometry().shape[0]):
+        assert rel(wide.solve_panel(w.rhs, p), O.solve_panel(w.rhs, p)) < 1e-4, p
+    X, sto = O.solve(w.rhs, 20, 1e-6)
+    Xm = w.rhs.copy()
+    st = wide.Solve(Xm, 20, 1e-6)
+    assert st["converged"] and abs(st["iterations"] - sto["iterations"]) <= 2
+    assert rel(Xm, X) < 1e-4
