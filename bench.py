@@ -333,7 +333,10 @@ def gradient_arm(args, ws, local):
            "workload": args.grad_config, "grid": [w.disc.nx, w.disc.ny, w.disc.nz], "sources": k,
            "receivers": int(len(w.meta["receivers"])), "precision": "mixed",
            "step": "Initialize + forward solve + adjoint solve + gradient kernel",
-           "misfit": float(J), "gradient_norm": float(torch.linalg.norm(g))}
+           "misfit": float(J), "gradient_norm": float(torch.linalg.norm(g)),
+           # the misfit relative to the data's own energy, 0.5 ||d||^2
+           "relative_misfit": float(J) / (0.5 * float(torch.linalg.norm(data)) ** 2),
+           "data_norm": float(torch.linalg.norm(data))}
     H.Finalize()
     return out
 
@@ -648,6 +651,7 @@ def main():
     H.Solve(X0, RESTART, REL_TOL)
     mixed_block0 = X0.cpu().numpy().reshape(N, -1)
     del X0, mixed["X"]
+    torch.cuda.empty_cache()
     prof = profile_block(H, w, kb, stream)
     roof, other_roofs = roofline_from_profile(prof, peaks)
     launches_per_step = sum(v["launches"] for n, v in prof.items() if n != "sweep")

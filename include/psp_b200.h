@@ -150,6 +150,29 @@ int psp_cu_gradient_device(psp_cu_handle* h, const double* d_U, const double* d_
 /* B := T_p B on panel p only (SolvePanel, solve.hpp:736-882); host grid. */
 int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel);
 
+/* z-panel pipeline over several GPUs (the one-process form of the
+ * reference's panel distribution: SubdiagonalUpdate / MultiplySuperdiagonal,
+ * solve.hpp:884-948, 969-1047, and the panel-local factorizations of
+ * initialize_finalize.hpp:123-322).  A rank's handle factors only panels
+ * [p0, p1) (call before its first Initialize); its vectors are slabs of the
+ * grid, planes z_base .. of nx*ny*k complex entries each.
+ *
+ * psp_cu_solve_panel_slab: SolvePanel (solve.hpp:736-882) of panel `panel`
+ * on a device slab, in place.  in_mode 0: B_i := T_i B_i; 1: B_i := T_i (B_i
+ * - A_{i,i-1} B_{i-1}), reading the plane below the panel; 2: B_i := T_i
+ * (-A_{i,i+1} B_{i+1}), reading the plane above it; out_accumulate adds the
+ * result to B_i instead of replacing it.
+ *
+ * psp_cu_multiply_slab: Y := A X, or Y := Bv - A X when Bv is not NULL, on
+ * planes [z_first, z_first + z_count) of device slabs X, Y, Bv whose first
+ * stored plane is z_slab; X must hold the planes next to that range that
+ * exist in the grid (the halo). */
+int psp_cu_set_panel_range(psp_cu_handle* h, int p0, int p1);
+int psp_cu_solve_panel_slab(psp_cu_handle* h, double* d_B, int k, int panel, int in_mode, int out_accumulate,
+                            int z_base);
+int psp_cu_multiply_slab(psp_cu_handle* h, const double* d_X, double* d_Y, const double* d_Bv, int k, int z_first,
+                         int z_count, int z_slab);
+
 /* Cap on GMRES inner steps (0 = none, the reference behaviour). */
 int psp_cu_set_max_iterations(psp_cu_handle* h, int max_iterations);
 
@@ -185,6 +208,11 @@ int psp_cu_hessenberg_eigenvalues(int n, const double* H, int ldh, double* w);
  * (lowest v, depth, padding, class) as in main.hpp:728-821. */
 int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info);
 
+/* The same panel geometry from a discretization alone (host only, no
+ * handle or GPU): number of panels and, if info != NULL, 4 ints per panel
+ * (lowest v, depth, padding, class), main.hpp:12-57, 728-821. */
+int psp_cu_panel_geometry(const psp_cu_disc* disc, int planes_per_panel, int* num_panels, int* info);
+
 /* Seconds spent in the last Initialize and bytes of stored panel factors. */
 int psp_cu_setup_info(const psp_cu_handle* h, double* setup_seconds, long long* factor_bytes);
 
@@ -206,6 +234,13 @@ int psp_cu_memory_info(const psp_cu_handle* h, int* resident_panels, int* num_pa
  * the factors, else the width of the equal blocks it solves one after
  * another (no counterpart in the reference, which holds all k at once). */
 int psp_cu_solve_block_width(psp_cu_handle* h, int k, int m, int* width);
+
+/* Host-only form of the same choice for given sizes: the GMRES block width
+ * for k right-hand sides when avail_bytes of device memory are left and one
+ * right-hand side's workspace takes per_rhs_bytes (cap > 0 limits it).
+ * PSP_CU_OUT_OF_MEMORY, with both sizes in the message, when not even one
+ * fits. */
+int psp_cu_plan_block_width(int k, double avail_bytes, double per_rhs_bytes, int cap, int* width);
 
 /* The CUDA stream (cudaStream_t) all work of the handle is issued on. */
 int psp_cu_get_stream(const psp_cu_handle* h, void** stream);

@@ -75,7 +75,8 @@ C_ABI_SYMBOLS = [
     "psp_cu_multiply_device_noalloc", "psp_cu_gradient_device", "psp_cu_initialize_batch", "psp_cu_solve_batch",
     "psp_cu_grid_load", "psp_cu_grid_interpolate", "psp_cu_grid_write_plane", "psp_cu_grid_write_volume",
     "psp_cu_set_view_iterates", "psp_cu_set_ritz_values", "psp_cu_get_ritz_values", "psp_cu_hessenberg_eigenvalues",
-    "psp_cu_memory_info", "psp_cu_solve_block_width",
+    "psp_cu_memory_info", "psp_cu_solve_block_width", "psp_cu_plan_block_width",
+    "psp_cu_set_panel_range", "psp_cu_solve_panel_slab", "psp_cu_multiply_slab", "psp_cu_panel_geometry",
 ]
 
 PROFILE_CATEGORIES = ["factor_gemm", "solve_gemm", "ldl_diag", "ldl_trsm", "assemble", "extend_add",
@@ -134,6 +135,11 @@ def lib():
         L.psp_cu_get_ritz_values.argtypes = [vp, ip, ip, dp]
         L.psp_cu_hessenberg_eigenvalues.argtypes = [ci, dp, ci, dp]
         L.psp_cu_solve_block_width.argtypes = [vp, ci, ci, ip]
+        L.psp_cu_plan_block_width.argtypes = [ci, ctypes.c_double, ctypes.c_double, ci, ip]
+        L.psp_cu_set_panel_range.argtypes = [vp, ci, ci]
+        L.psp_cu_panel_geometry.argtypes = [ctypes.POINTER(_Disc), ci, ip, ip]
+        L.psp_cu_solve_panel_slab.argtypes = [vp, vp, ci, ci, ci, ci, ci]
+        L.psp_cu_multiply_slab.argtypes = [vp, vp, vp, vp, ci, ci, ci, ci]
         L.psp_cu_memory_info.argtypes = [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
@@ -285,6 +291,26 @@ def hessenberg_eigenvalues(H):
     _check(lib().psp_cu_hessenberg_eigenvalues(n, _dptr(A.reshape(-1, order="F").view(np.float64)), max(n, 1),
                                                _dptr(w.view(np.float64))))
     return w
+
+
+def panel_geometry(disc, planes_per_panel=4):
+    """Panel split of ``disc`` (host only): int array (num_panels, 4) of
+    (lowest v, depth, padding, class) per panel, v = nz - 1 - z."""
+    d = disc._c()
+    n = ctypes.c_int()
+    _check(lib().psp_cu_panel_geometry(ctypes.byref(d), int(planes_per_panel), ctypes.byref(n), None))
+    info = np.zeros(4 * n.value, dtype=np.int32)
+    _check(lib().psp_cu_panel_geometry(ctypes.byref(d), int(planes_per_panel), ctypes.byref(n), _iptr(info)))
+    return info.reshape(n.value, 4)
+
+
+def plan_block_width(k, avail_bytes, per_rhs_bytes, cap=0):
+    """GMRES block width for k right-hand sides given the device bytes left
+    and one right-hand side's workspace (psp_cu_plan_block_width; host only)."""
+    wd = ctypes.c_int()
+    _check(lib().psp_cu_plan_block_width(int(k), float(avail_bytes), float(per_rhs_bytes), int(cap),
+                                         ctypes.byref(wd)))
+    return wd.value
 
 
 def analyze_class(disc, planes_per_panel=4, cutoff=12, cls=0):
@@ -518,6 +544,23 @@ class DistHelmholtz:
         f, b = ctypes.c_double(), ctypes.c_double()
         _check(lib().psp_cu_sweep_cost(self._h, int(k), ctypes.byref(f), ctypes.byref(b)))
         return f.value, b.value
+
+    def set_panel_range(self, p0, p1):
+        """Factor only panels [p0, p1) (a z-panel pipeline rank); before the
+        first Initialize."""
+        _check(lib().psp_cu_set_panel_range(self._h, int(p0), int(p1)))
+
+    def solve_panel_slab(self, B, k, panel, in_mode, out_accumulate, z_base):
+        """SolvePanel on a CUDA complex128 slab of planes z_base.. (in place)."""
+        _check(lib().psp_cu_solve_panel_slab(self._h, ctypes.c_void_p(B.data_ptr()), int(k), int(panel),
+                                             int(in_mode), int(out_accumulate), int(z_base)))
+
+    def multiply_slab(self, X, Y, k, z_first, z_count, z_slab, Bv=None):
+        """Y := A X (or Bv - A X) on planes [z_first, z_first + z_count) of
+        CUDA complex128 slabs whose first stored plane is z_slab."""
+        _check(lib().psp_cu_multiply_slab(self._h, ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(Y.data_ptr()),
+                                          ctypes.c_void_p(Bv.data_ptr()) if Bv is not None else None, int(k),
+                                          int(z_first), int(z_count), int(z_slab)))
 
     def multiply_device(self, B):
         _check(lib().psp_cu_multiply_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))

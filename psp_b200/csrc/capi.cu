@@ -223,6 +223,30 @@ int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel) {
     });
 }
 
+int psp_cu_set_panel_range(psp_cu_handle* h, int p0, int p1) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] { h->solver->SetPanelRange(p0, p1); });
+}
+
+int psp_cu_solve_panel_slab(psp_cu_handle* h, double* d_B, int k, int panel, int in_mode, int out_accumulate,
+                            int z_base) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!d_B) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
+        h->solver->SolvePanelSlab(reinterpret_cast<psp_b200::z64*>(d_B), k, panel, in_mode, out_accumulate, z_base);
+    });
+}
+
+int psp_cu_multiply_slab(psp_cu_handle* h, const double* d_X, double* d_Y, const double* d_Bv, int k, int z_first,
+                         int z_count, int z_slab) {
+    if (int e = CheckHandle(h)) return e;
+    return Guard([&] {
+        if (!d_X || !d_Y) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
+        h->solver->MultiplySlab(reinterpret_cast<const psp_b200::z64*>(d_X), reinterpret_cast<psp_b200::z64*>(d_Y),
+                                reinterpret_cast<const psp_b200::z64*>(d_Bv), k, z_first, z_count, z_slab);
+    });
+}
+
 int psp_cu_set_max_iterations(psp_cu_handle* h, int max_iterations) {
     if (int e = CheckHandle(h)) return e;
     h->solver->SetMaxIterations(max_iterations);
@@ -274,6 +298,27 @@ int psp_cu_geometry(const psp_cu_handle* h, int* num_panels, int* info) {
             info[4 * p + 3] = g.Class(p);
         }
     return PSP_CU_OK;
+}
+
+int psp_cu_panel_geometry(const psp_cu_disc* disc, int planes_per_panel, int* num_panels, int* info) {
+    if (!disc) {
+        g_lastError = "null argument";
+        return PSP_CU_LOGIC_ERROR;
+    }
+    return Guard([&] {
+        psp_b200::DiscParams d;
+        std::memcpy(&d, disc, sizeof(d));
+        psp_b200::PanelGeometry g;
+        g.Init(d, planes_per_panel);
+        if (num_panels) *num_panels = g.numPanels;
+        if (info)
+            for (int p = 0; p < g.numPanels; ++p) {
+                info[4 * p + 0] = g.LowV(p);
+                info[4 * p + 1] = g.Depth(p);
+                info[4 * p + 2] = g.Padding(p);
+                info[4 * p + 3] = g.Class(p);
+            }
+    });
 }
 
 int psp_cu_get_stream(const psp_cu_handle* h, void** stream) {
@@ -368,6 +413,13 @@ int psp_cu_solve_block_width(psp_cu_handle* h, int k, int m, int* width) {
         if (!width) throw PspError(PSP_CU_LOGIC_ERROR, "null output");
         CUDA_CHECK(cudaSetDevice(h->solver->device()));
         *width = h->solver->SolveBlockWidth(k, m);
+    });
+}
+
+int psp_cu_plan_block_width(int k, double avail_bytes, double per_rhs_bytes, int cap, int* width) {
+    return Guard([&] {
+        if (!width) throw PspError(PSP_CU_LOGIC_ERROR, "null output");
+        *width = psp_b200::ChooseBlockWidth(k, avail_bytes, per_rhs_bytes, cap);
     });
 }
 

@@ -41,9 +41,9 @@ constexpr int kApplyTX = 64;
 __global__ void __launch_bounds__(kThreads) helmholtz_apply_kernel(const z64* __restrict__ x, z64* __restrict__ y,
                                                                    const z64* __restrict__ b,
                                                                    const double* __restrict__ vel, StencilParams sp,
-                                                                   int k) {
+                                                                   int k, int zFirst, int zSlab) {
     __shared__ z64 coef[kApplyTX][7];
-    const int x0 = blockIdx.x * kApplyTX, yy = blockIdx.y, zz = blockIdx.z;
+    const int x0 = blockIdx.x * kApplyTX, yy = blockIdx.y, zz = zFirst + (int)blockIdx.z;
     const int nx = sp.nx, ny = sp.ny, nz = sp.nz;
     const int64_t nxy = (int64_t)nx * ny;
     const int npts = min(kApplyTX, nx - x0);
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(kThreads) helmholtz_apply_kernel(const z64* __
         coef[threadIdx.x][6] = -t.vR;
     }
     __syncthreads();
-    const int64_t base = x0 + yy * (int64_t)nx + zz * nxy;
+    const int64_t base = x0 + yy * (int64_t)nx + (zz - zSlab) * nxy;  // storage: planes from zSlab
     const int64_t sx = k, sy = (int64_t)nx * k, sz = nxy * k;
     for (int e = threadIdx.x; e < npts * k; e += blockDim.x) {
         const int p = e / k, r = e - p * k;
@@ -439,7 +439,14 @@ void LaunchGemmCfg(const GemmOp<R>* ops, const GemmTile* tiles, int numTiles, cu
 void LaunchHelmholtzApply(const z64* x, z64* y, const z64* b, const double* vel, const StencilParams& sp, int k,
                           cudaStream_t st) {
     dim3 grid(CeilDiv(sp.nx, kApplyTX), sp.ny, sp.nz);
-    helmholtz_apply_kernel<<<grid, kThreads, 0, st>>>(x, y, b, vel, sp, k);
+    helmholtz_apply_kernel<<<grid, kThreads, 0, st>>>(x, y, b, vel, sp, k, 0, 0);
+    CUDA_LAUNCH_CHECK();
+}
+
+void LaunchHelmholtzApplyPlanes(const z64* x, z64* y, const z64* b, const double* vel, const StencilParams& sp,
+                                int k, int zFirst, int zCount, int zSlab, cudaStream_t st) {
+    dim3 grid(CeilDiv(sp.nx, kApplyTX), sp.ny, zCount);
+    helmholtz_apply_kernel<<<grid, kThreads, 0, st>>>(x, y, b, vel, sp, k, zFirst, zSlab);
     CUDA_LAUNCH_CHECK();
 }
 

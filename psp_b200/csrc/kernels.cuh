@@ -27,6 +27,10 @@ struct StencilParams {
 // FormGlobalRow, initialize_finalize.hpp:527-587, evaluated on the fly).
 void LaunchHelmholtzApply(const z64* x, z64* y, const z64* b, const double* vel, const StencilParams& sp, int k,
                           cudaStream_t st);
+// The same on planes [zFirst, zFirst + zCount) of slabs whose first stored
+// plane is zSlab (x must hold the existing planes next to the range).
+void LaunchHelmholtzApplyPlanes(const z64* x, z64* y, const z64* b, const double* vel, const StencilParams& sp,
+                                int k, int zFirst, int zCount, int zSlab, cudaStream_t st);
 
 // grad[i] (+)= -Re( dA_ii/dvel_i * sum_r Z[i,r] U[i,r] ) for natural-order
 // [N][k] grids: the velocity gradient of a real misfit whose forward fields

@@ -169,7 +169,9 @@ public:
     // Makes panel p's factors available: a recomputed panel is factored
     // into its class's slot unless the slot holds it already.
     void EnsurePanel(int p);
-    void SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc);
+    // Panel p's solve on grid B (rows of ldk complex entries per point);
+    // B's first stored plane is z = zBase (a slab of the global grid).
+    void SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc, int zBase = 0);
     // One sweep (Precondition); replayed from a captured CUDA graph when
     // `useGraph` and profiling is off.
     void Sweep(z64* B, int ldk, int k, bool useGraph);
@@ -252,6 +254,7 @@ private:
     std::vector<int64_t> gOff_, dOff_;    // per (panel, node): offset in its panel's storage
     std::vector<cpx<R>*> gPtr_, dPtr_;     // per (panel, node): where G and D live
     std::vector<char> resident_;           // per panel
+    std::vector<char> owned_;              // per panel: inside the handle's panel range
     std::vector<FactorFront<R>> fronts_;   // per (panel, node), transient pointers unset
     // Recomputed panels: one slot per class for G and D, the arena of their
     // factorization transients, their programs and what each slot holds.
@@ -260,8 +263,8 @@ private:
     int slotHolds_[3] = {-1, -1, -1};
     int64_t refactors_ = 0;
     bool AllResident() const {
-        for (char r : resident_)
-            if (!r) return false;
+        for (size_t p = 0; p < resident_.size(); ++p)
+            if (owned_[p] && !resident_[p]) return false;
         return true;
     }
     std::vector<std::vector<int>> depthNodes_;
@@ -397,12 +400,18 @@ void FactorStore<R>::BuildLayout() {
     const double reserveRhs = (double)EnvInt("PSP_B200_SOLVE_RESERVE_RHS", 16);
     const double reserve = reserveRhs * (double)h_.NumUnknowns() * sizeof(z64) * 25 + 1.0e9 + 0.02 * totalB;
     const long long cap = EnvInt("PSP_B200_RESIDENT_PANELS", -1);
+    // panels of the handle's range only (a z-panel pipeline rank): the
+    // others have no factors here
+    owned_.assign(np, 0);
+    for (int p = std::max(0, h_.panelBegin_); p < std::min(np, h_.panelEnd_); ++p) owned_[p] = 1;
     std::vector<int> order;  // residency priority
-    order.push_back(np - 1);
-    for (int p = 0; p < np - 1; ++p) order.push_back(p);
-    resident_.assign(np, 1);
+    if (owned_[np - 1]) order.push_back(np - 1);
+    for (int p = 0; p < np - 1; ++p)
+        if (owned_[p]) order.push_back(p);
+    resident_ = owned_;
     double all = 0;
-    for (int p = 0; p < np; ++p) all += (double)panelBytes(p);
+    for (int p = 0; p < np; ++p)
+        if (owned_[p]) all += (double)panelBytes(p);
     if (cap >= 0 || all > avail - reserve) {
         // room for the slots and the recompute arena of every class that
         // may lose a panel (all classes but the top panel's, unless capped
@@ -413,7 +422,7 @@ void FactorStore<R>::BuildLayout() {
             std::vector<int> one;
             int64_t pb = 0;
             for (int p = 0; p < np; ++p)
-                if (g.Class(p) == c && (p != np - 1 || cap == 0)) {
+                if (owned_[p] && g.Class(p) == c && (p != np - 1 || cap == 0)) {
                     if (one.empty()) one.push_back(p);
                     pb = std::max(pb, panelBytes(p));
                 }
@@ -446,7 +455,7 @@ void FactorStore<R>::BuildLayout() {
     int64_t slotBytesG[3] = {0, 0, 0}, slotBytesD[3] = {0, 0, 0};
     std::vector<int> recomputed[3];
     for (int p = 0; p < np; ++p)
-        if (!resident_[p]) {
+        if (owned_[p] && !resident_[p]) {
             const int c = g.Class(p);
             slotBytesG[c] = std::max(slotBytesG[c], gPanel[p]);
             slotBytesD[c] = std::max(slotBytesD[c], dPanel[p]);
@@ -465,6 +474,7 @@ void FactorStore<R>::BuildLayout() {
     dPtr_.assign((size_t)np * nn_, nullptr);
     for (int p = 0; p < np; ++p) {
         const int c = g.Class(p);
+        if (!owned_[p]) continue;
         cpx<R>* gp = resident_[p] ? G_.as<cpx<R>>() + gBase[p] : slotG_[c].template as<cpx<R>>();
         cpx<R>* dp = resident_[p] ? D_.as<cpx<R>>() + dBase[p] : slotD_[c].template as<cpx<R>>();
         for (int t = 0; t < nn_; ++t) {
@@ -499,7 +509,7 @@ void FactorStore<R>::BuildLayout() {
     recompute_.clear();
     recompute_.resize(np);
     for (int p = 0; p < np; ++p)
-        if (!resident_[p])
+        if (owned_[p] && !resident_[p])
             recompute_[p] = FactorGroup({p}, rarena_.template as<unsigned char>(), rarena_.bytes);
     layout_ = true;
 }
@@ -893,7 +903,7 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             f.ldg = GLeadingDim(f.s, f.u);
             f.tmap = nullptr;
             if constexpr (std::is_same<R, float>::value) {
-                if (tc_ && f.s > 0) {
+                if (tc_ && f.s > 0 && owned_[p]) {
                     const size_t i = (size_t)p * nn_ + t;
                     EncodeSweepTcMaps(f, P.mapsHost[i].b);
                     f.tmap = P.maps.template as<unsigned char>() + i * sizeof(typename SolvePlan::MapPair);
@@ -1130,7 +1140,7 @@ bool FactorStore<R>::Autotune(SolvePlan& P) {
         for (int c = 0; c < 3; ++c) {
             int p = -1;
             for (int q = 0; q < g.numPanels && p < 0; ++q)
-                if (g.Class(q) == c) p = q;
+                if (g.Class(q) == c && owned_[q]) p = q;
             if (p < 0) continue;
             ClassPlan& cp = P.cplan[c];
             size_t maxVar = 0;
@@ -1194,7 +1204,8 @@ bool FactorStore<R>::Autotune(SolvePlan& P) {
 }
 
 template <typename R>
-void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc) {
+void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int outAcc, int zBase) {
+    if (!owned_[p]) throw PspError(kLogicError, "panel " + std::to_string(p) + " is outside the handle's panel range");
     SolvePlan& P = Plan(k);
     EnsurePanel(p);
     const PanelGeometry& g = an_.geom;
@@ -1205,7 +1216,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
     io.ndToNat = h_.dNdToNat_[c].as<int>();
     io.nx = an_.disc.nx;
     io.nxy = an_.disc.nx * an_.disc.ny;
-    io.nz = an_.disc.nz;
+    io.nz = an_.disc.nz - zBase;  // kernels index plane nz - 1 - v: relative to the slab's first plane
     io.ldk = ldk;
     io.padding = g.Padding(p);
     io.vOffset = g.SubVOffset(p);
@@ -1575,6 +1586,39 @@ void Helmholtz::SolvePanelDevice(z64* B, int k, int panel) {
     CUDA_CHECK(cudaStreamSynchronize(stream_));
 }
 
+void Helmholtz::SetPanelRange(int p0, int p1) {
+    if (f64_ || f32_) throw PspError(kLogicError, "the panel range must be set before the first Initialize");
+    if (p0 < 0 || p1 > an_.geom.numPanels || p0 >= p1) throw PspError(kLogicError, "invalid panel range");
+    panelBegin_ = p0;
+    panelEnd_ = p1;
+}
+
+void Helmholtz::SolvePanelSlab(z64* B, int k, int panel, int inMode, int outAccumulate, int zBase) {
+    if (!initialized_) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    if (panel < 0 || panel >= an_.geom.numPanels) throw PspError(kLogicError, "panel index out of range");
+    if (inMode < 0 || inMode > 2 || k < 1 || zBase < 0 || zBase >= an_.disc.nz)
+        throw PspError(kLogicError, "invalid panel-solve arguments");
+    CUDA_CHECK(cudaSetDevice(device_));
+    ProfilerBinding bind(&prof_);
+    const int w = RhsBlockWidth(k);
+    for (int r0 = 0; r0 < k; r0 += w) {
+        const int kb = std::min(w, k - r0);
+        if (f64_) f64_->SolvePanel(B + r0, k, kb, panel, inMode, outAccumulate, zBase);
+        else f32_->SolvePanel(B + r0, k, kb, panel, inMode, outAccumulate, zBase);
+    }
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+    CheckSweepStatus();
+}
+
+void Helmholtz::MultiplySlab(const z64* X, z64* Y, const z64* Bv, int k, int zFirst, int zCount, int zSlab) {
+    if (!dVel_.p) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
+    if (k < 1 || zCount < 1 || zFirst < 0 || zFirst + zCount > an_.disc.nz || zSlab > zFirst || zSlab < 0)
+        throw PspError(kLogicError, "invalid slab multiply arguments");
+    CUDA_CHECK(cudaSetDevice(device_));
+    LaunchHelmholtzApplyPlanes(X, Y, Bv, dVel_.as<double>(), sp_, k, zFirst, zCount, zSlab, stream_);
+    CUDA_CHECK(cudaStreamSynchronize(stream_));
+}
+
 void Helmholtz::MultiplyDevice(z64* B, int k) {
     if (!dVel_.p) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
     CUDA_CHECK(cudaSetDevice(device_));
@@ -1646,23 +1690,16 @@ double Helmholtz::GmresBytesPerRhs(int m) const {
     return (double)NumUnknowns() * sizeof(z64) * (m + 6) + plan;
 }
 
-int Helmholtz::GmresBlockWidth(int k, int m) {
-    int cap = k;
-    const long long env = EnvInt("PSP_B200_MAX_RHS_BLOCK", 0);
-    if (env > 0) cap = (int)std::min<long long>(cap, env);
-    size_t freeB = 0, totalB = 0;
-    CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
-    // the scratch is reused for the workspace; the plan of the current width
-    // (when built) is already counted as used memory
-    const double avail = (double)freeB + (double)pool_.bytes - 0.5e9;
-    const double perRhs = GmresBytesPerRhs(m);
-    const double fitD = std::floor(0.95 * avail / perRhs);
+int ChooseBlockWidth(int k, double availBytes, double perRhsBytes, int cap) {
+    if (k < 1 || perRhsBytes <= 0) throw PspError(kLogicError, "need k >= 1 and a positive workspace size");
+    const double fitD = std::floor(0.95 * availBytes / perRhsBytes);
     if (fitD < 1)
         throw PspError(kOutOfMemory, "the GMRES workspace of one right-hand side (" +
-                                         std::to_string(perRhs / 1e9) + " GB at restart " + std::to_string(m) +
-                                         ") does not fit in the " + std::to_string(avail / 1e9) +
+                                         std::to_string(perRhsBytes / 1e9) + " GB) does not fit in the " +
+                                         std::to_string(availBytes / 1e9) +
                                          " GB of device memory left beside the factors");
-    const int fit = (int)std::min<double>(fitD, cap);
+    int fit = (int)std::min<double>(fitD, k);
+    if (cap > 0) fit = std::min(fit, cap);
     const int nb = (k + fit - 1) / fit;
     int kb = (k + nb - 1) / nb;
     // whole 16-column sweep tiles when that still fits
@@ -1671,6 +1708,16 @@ int Helmholtz::GmresBlockWidth(int k, int m) {
         if (up <= fit && up < k) kb = up;
     }
     return std::max(1, kb);
+}
+
+int Helmholtz::GmresBlockWidth(int k, int m) {
+    const long long cap = EnvInt("PSP_B200_MAX_RHS_BLOCK", 0);
+    size_t freeB = 0, totalB = 0;
+    CUDA_CHECK(cudaMemGetInfo(&freeB, &totalB));
+    // the scratch is reused for the workspace; the plan of the current width
+    // (when built) is already counted as used memory
+    const double avail = (double)freeB + (double)pool_.bytes - 0.5e9;
+    return ChooseBlockWidth(k, avail, GmresBytesPerRhs(m), cap > 0 ? (int)std::min<long long>(cap, k) : 0);
 }
 
 void Helmholtz::SolveDevice(z64* B, int k, int m, double relTol, SolveStats* stats) {

@@ -60,6 +60,13 @@ struct SolveStats {
 template <typename R>
 class FactorStore;
 
+// GMRES block width for k right-hand sides when availBytes of device memory
+// are left and one right-hand side's workspace takes perRhsBytes: the
+// widest that fits (at most cap when cap > 0), made equal across blocks and,
+// from 16 up, a multiple of 16 when that still fits.  Throws out-of-memory
+// with both sizes in the message when not even one fits.
+int ChooseBlockWidth(int k, double availBytes, double perRhsBytes, int cap);
+
 // Makes `p` the profiler of launches issued by this thread while in scope.
 struct ProfilerBinding {
     Profiler* prev;
@@ -129,6 +136,20 @@ public:
     // Panel factorizations run by sweeps since Initialize (recomputed panels).
     int64_t Refactorizations() const;
 
+    // z-panel pipeline ranks: only panels [p0, p1) are factored by this
+    // handle (set before its first Initialize); panel solves of the others
+    // are refused.
+    void SetPanelRange(int p0, int p1);
+    // Panel p's solve on a slab of the grid whose first stored plane is z =
+    // zBase (inMode / outAccumulate as in the sweep: 0 B_i; 1 B_i - A_{i,i-1}
+    // B_{i-1}, reading the plane below the panel; 2 -A_{i,i+1} B_{i+1}
+    // only, reading the plane above; outAccumulate adds the result).
+    void SolvePanelSlab(z64* B, int k, int panel, int inMode, int outAccumulate, int zBase);
+    // Y := A X (or Y := Bv - A X when Bv is given) on planes [zFirst, zFirst +
+    // zCount) of slabs X, Y (and Bv) whose first stored plane is zSlab; X
+    // must hold the planes next to that range that exist in the grid.
+    void MultiplySlab(const z64* X, z64* Y, const z64* Bv, int k, int zFirst, int zCount, int zSlab);
+
     // Right-hand sides per GMRES block a Solve of k sides with restart m
     // would use now (k when they all fit).
     int SolveBlockWidth(int k, int m) {
@@ -154,6 +175,7 @@ public:
     Analysis an_;
     double damping_;
     int device_;
+    int panelBegin_ = 0, panelEnd_ = 1 << 30;  // panel range of a pipeline rank
     cudaStream_t stream_ = nullptr;
 
 private:

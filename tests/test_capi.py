@@ -76,3 +76,23 @@ def test_grid_local_index_and_orders():
     for order, stored in layouts.items():
         h = P.DistUniformGrid.from_order(stored.ravel(), 4, 3, 2, 3, order)
         assert np.array_equal(h.data, ref), order
+
+
+def test_gmres_block_width_choice():
+    """The GMRES block width for the memory left (host-only form of the
+    choice Solve makes): all right-hand sides when they fit; otherwise equal
+    blocks as wide as fit, rounded up to whole 16-column sweep tiles when
+    that still fits; the environment-style cap; out-of-memory, with the
+    sizes, when not even one right-hand side fits."""
+    GB = 1e9
+    per = 2.6 * GB
+    assert P.plan_block_width(16, 100 * GB, per) == 16
+    assert P.plan_block_width(64, 96 * GB, per) == 32          # fit 35: two blocks of 32
+    assert P.plan_block_width(64, 80 * GB, per) == 22          # fit 29: three blocks of 22 (32 does not fit)
+    assert P.plan_block_width(64, 60 * GB, per) == 16          # fit 21: four blocks of 16
+    assert P.plan_block_width(3, 100 * GB, per, cap=2) == 2    # blocks of 2 (the last padded)
+    assert P.plan_block_width(5, 3 * GB, per) == 1
+    with pytest.raises(P.CudaError, match="does not fit"):
+        P.plan_block_width(4, 2 * GB, per)
+    with pytest.raises(P.LogicError):
+        P.plan_block_width(0, 100 * GB, per)

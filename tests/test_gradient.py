@@ -150,3 +150,30 @@ def test_autograd_gradient_matches_finite_differences_layered(product_lib):
     err_mixed = np.max(np.abs(gm[voxels] - fd) / np.maximum(np.abs(fd), 1e-2 * gmax))
     print("mixed-precision gradient vs finite differences: max relative error %.2e" % err_mixed)
     assert err_mixed < 1e-3
+
+
+@pytest.mark.gpu
+def test_gradient_with_recomputed_panels_matches_resident(product_lib, monkeypatch):
+    """When the factors do not fit (forced here by capping the resident
+    panels) the adjoint solve recomputes panels as the forward solve does:
+    the gradient equals the one from resident factors."""
+    import torch
+    import psp_b200 as P
+    from psp_b200.autograd import misfit_and_gradient
+    w, d, vel, f_np, receivers, data = _misfit_case()
+    v = torch.from_numpy(vel.reshape(-1).copy()).cuda()
+    f = torch.from_numpy(f_np).cuda()
+    recv, dat = torch.from_numpy(receivers).cuda(), torch.from_numpy(data).cuda()
+    grads = []
+    for cap in (None, "1"):
+        if cap is None:
+            monkeypatch.delenv("PSP_B200_RESIDENT_PANELS", raising=False)
+        else:
+            monkeypatch.setenv("PSP_B200_RESIDENT_PANELS", cap)
+        H = P.DistHelmholtz(d)
+        J, g = misfit_and_gradient(H, v, f, recv, dat, m=60, rel_tol=1e-11, precision=P.FP64)
+        info = H.memory_info()
+        assert (info["resident_panels"] == 1) == (cap is not None)
+        assert (info["refactorizations"] > 0) == (cap is not None)
+        grads.append(g.cpu().numpy())
+    assert np.linalg.norm(grads[1] - grads[0]) <= 1e-10 * np.linalg.norm(grads[0])

@@ -93,14 +93,18 @@ def test_mixed_route_solve_converges(setup):
         assert rel(Xm, X) < 1e-4, name
 
 
-def test_wide_tensor_core_tiles_match(product_lib):
-    """More than 16 right-hand sides: the tensor-core tiles take 32 (each G
-    stage split once for all of them; k = 40 leaves a partly filled last
-    tile, and the small fronts' short K-chunks exercise the split-K
-    reduction per 16-column sub-tile).  The preconditioner and every panel
-    solve agree with the CUDA-core kernels and the oracle, and a mixed
-    solve converges like the oracle's."""
-    w = W.small_case(**dict(CASE, k=40))
+@pytest.mark.parametrize("k", [16, 32, 40])
+def test_wide_tensor_core_tiles_match(product_lib, k):
+    """Tile widths and right-hand-side copies of the tensor-core kernels:
+    more than 16 right-hand sides take 32-wide tiles (each G stage split
+    once for all of them); when a tile spans every right-hand side (k = 16,
+    32) a stage's right-hand-side rows arrive by one bulk copy with the G
+    stage, otherwise (k = 40: a full and a partly filled tile) by per-thread
+    copies; the small fronts' short K-chunks exercise the split-K reduction
+    per 16-column sub-tile.  The preconditioner and every panel solve agree
+    with the CUDA-core kernels and the oracle, and a mixed solve converges
+    like the oracle's."""
+    w = W.small_case(**dict(CASE, k=k))
     O = oracle_for(w.disc)
     O.initialize(w.velocity)
     wide = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": "0", "PSP_B200_SWEEP_CUDA_CORES": None})
