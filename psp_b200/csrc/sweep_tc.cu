@@ -313,8 +313,22 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
     const int rowEntries = kFwd ? 3 * k : k;  // complex entries of one B row
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
+    // Right-hand sides come from the preceding kernels: the B copies of the
+    // stages issued before that kernel has finished (the first ring's worth;
+    // their G copies go out at once) wait for it.
+    bool ready = !bulkB;
+    int pending = 0;
+    const c32* pendSrc[kRawMax];
+    uint32_t pendBytes[kRawMax];
+    auto flush = [&] {
+        PdlWait();
+        for (int i = 0; i < pending; ++i)
+            if (pendBytes[i]) umma::BulkCopy(bslots + i * C::OwnSlot(kFwd), pendSrc[i], pendBytes[i], &S.rawFull[i]);
+        ready = true;
+    };
     for (int g = 0; cur.Valid(g); ++g) {
         const int slot = g % C::RawSlots(kFwd);
+        if (!ready && g == C::RawSlots(kFwd)) flush();
         if (g >= C::RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / C::RawSlots(kFwd)) - 1) & 1, S, status)) return;
         const LoadMeta& m = cur.m;
         const int kBase = cur.KBase();
@@ -324,9 +338,15 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
         const int brows = bulkB ? max(0, min(kStageK, m.ke - kBase)) : 0;
         const uint32_t bbytes = (uint32_t)brows * rowEntries * 8u;
         umma::MbarArriveExpectTx(&S.rawFull[slot], kRawA + bbytes);
-        if (bbytes)
-            umma::BulkCopy(bslots + slot * C::OwnSlot(kFwd), m.B + (int64_t)kBase * rowEntries, bbytes,
-                           &S.rawFull[slot]);
+        if (ready) {
+            if (bbytes)
+                umma::BulkCopy(bslots + slot * C::OwnSlot(kFwd), m.B + (int64_t)kBase * rowEntries, bbytes,
+                               &S.rawFull[slot]);
+        } else {  // g == slot here
+            pendSrc[pending] = m.B + (int64_t)kBase * rowEntries;
+            pendBytes[pending] = bbytes;
+            ++pending;
+        }
         const unsigned char* map = reinterpret_cast<const unsigned char*>(m.tmap) + (kFwd ? 0 : 128);
         if (kFwd)
             umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, m.row0, kBase, &S.rawFull[slot]);
@@ -334,6 +354,7 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
             umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, kBase, m.row0, &S.rawFull[slot]);
         cur.Advance();
     }
+    if (!ready) flush();
 }
 
 // ------------------------------------------------------------------ converters
@@ -855,15 +876,12 @@ void PrepareSweepTcKernels() {
                                     (int)Cfg<32>::kSmem));
 }
 
-// B rows of a stage are contiguous (one bulk copy) when a tile spans every
-// right-hand side, and 16-byte aligned when k is even (the front work
-// vectors then start on 16-byte boundaries).
-static int BulkB(int k, int cols) { return (k <= cols && k % 2 == 0) ? 1 : 0; }
+bool SweepTcBulkB(int k, int cols) { return k <= cols && k % 2 == 0; }
 
-void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols,
+void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols, bool bulk,
                           const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    const int bulkB = BulkB(k, cols);
+    const int bulkB = bulk && SweepTcBulkB(k, cols) ? 1 : 0;
     if (cols == 32)
         LaunchPdl(sweep_tc_forward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles, n,
                   k, bulkB, w);
@@ -874,9 +892,9 @@ void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, i
 }
 
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k, int cols,
-                           const PanelIO& io, const SweepWork& w, cudaStream_t st) {
+                           bool bulk, const PanelIO& io, const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    const int bulkB = BulkB(k, cols);
+    const int bulkB = bulk && SweepTcBulkB(k, cols) ? 1 : 0;
     if (cols == 32)
         LaunchPdl(sweep_tc_backward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles,
                   n, B, k, bulkB, io, w);

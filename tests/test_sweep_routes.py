@@ -107,7 +107,8 @@ def test_wide_tensor_core_tiles_match(product_lib, k):
     w = W.small_case(**dict(CASE, k=k))
     O = oracle_for(w.disc)
     O.initialize(w.velocity)
-    wide = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": "0", "PSP_B200_SWEEP_CUDA_CORES": None})
+    mode = "bulk" if k in (16, 32) else "0"
+    wide = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": mode, "PSP_B200_SWEEP_CUDA_CORES": None})
     cc = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": None, "PSP_B200_SWEEP_CUDA_CORES": "1"})
     ref = O.precondition(w.rhs)
     x = wide.precondition(w.rhs)
