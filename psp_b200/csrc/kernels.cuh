@@ -236,16 +236,10 @@ void PrepareSweepTcKernels();
 // out (64-byte aligned host memory) for the front's G, s, u and ldg.
 constexpr size_t kSweepTcMapBytes = 256;
 void EncodeSweepTcMaps(const SweepFront<float>& f, void* out);
-// `bulk`: when SweepTcBulkB(k, cols) (a tile spans every right-hand side
-// and k is even, so a stage's right-hand-side rows are contiguous and
-// 16-byte aligned) they arrive by one bulk copy with the G stage, issued by
-// the producer once the preceding kernel has finished; otherwise every
-// converter thread copies its own entries.
-bool SweepTcBulkB(int k, int cols);
-void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols, bool bulk,
+void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols,
                           const SweepWork& w, cudaStream_t st);
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k, int cols,
-                           bool bulk, const PanelIO& io, const SweepWork& w, cudaStream_t st);
+                           const PanelIO& io, const SweepWork& w, cudaStream_t st);
 
 // ------------------------------------------------------------------ GMRES vectors
 

@@ -274,7 +274,6 @@ private:
     // and the K-chunk of its tiles.
     struct SweepVariant {
         bool tc = false;
-        bool bulk = false;      // tensor cores: right-hand-side stages by bulk copy
         int cols = kSweepCols;  // right-hand sides per tile (tensor cores: 16 or 32)
         int chunk = 0;
         size_t tiles = 0;  // arena offset of the tile list
@@ -986,19 +985,18 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // them (one split of each G stage for twice the columns); the 16-wide
     // default stays a candidate.
     auto makeVariants = [&](const ClassStructure& cs, int d, bool fwd, std::vector<SweepVariant>& out) {
-        struct Cand { bool tc; int cols, chunk; bool bulk; };
+        struct Cand { bool tc; int cols, chunk; };
         std::vector<Cand> cand;
         if (tc_) {
             const int wide = k > kSweepCols ? 32 : kSweepCols;
-            cand.push_back({true, wide, 0, false});
-            for (int kc : {64, 128, 256, 512}) cand.push_back({true, wide, kc, false});
-            if (wide != kSweepCols) cand.push_back({true, kSweepCols, 0, false});
-            if (SweepTcBulkB(k, wide))
-                for (int kc : {0, 256, 512}) cand.push_back({true, wide, kc, true});
-            cand.push_back({false, kSweepCols, 0, false});
-            for (int kc : {64, 128}) cand.push_back({false, kSweepCols, kc, false});
+            cand.push_back({true, wide, 0});
+            for (int kc : {64, 128, 256, 512}) cand.push_back({true, wide, kc});
+            if (wide != kSweepCols)
+                for (int kc : {0, 512}) cand.push_back({true, kSweepCols, kc});
+            cand.push_back({false, kSweepCols, 0});
+            for (int kc : {64, 128}) cand.push_back({false, kSweepCols, kc});
         } else {
-            cand.push_back({false, kSweepCols, 0, false});
+            cand.push_back({false, kSweepCols, 0});
         }
         std::vector<std::vector<SweepTile>> seen;
         for (const auto& cd : cand) {
@@ -1006,12 +1004,10 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
             SweepVariant v;
             v.tc = cd.tc;
             v.cols = cd.cols;
-            v.bulk = cd.bulk;
             v.chunk = makeTiles(cs, d, fwd, cd.tc, cd.cols, cd.chunk, tiles);
             bool dup = false;
             for (size_t i = 0; i < seen.size() && !dup; ++i)
-                dup = out[i].tc == v.tc && out[i].cols == v.cols && out[i].bulk == v.bulk &&
-                      seen[i].size() == tiles.size() &&
+                dup = out[i].tc == v.tc && out[i].cols == v.cols && seen[i].size() == tiles.size() &&
                       std::equal(tiles.begin(), tiles.end(), seen[i].begin(), [](const SweepTile& a, const SweepTile& b) {
                           return a.front == b.front && a.row0 == b.row0 && a.col0 == b.col0 && a.k0 == b.k0 &&
                                  a.k1 == b.k1;
@@ -1063,22 +1059,11 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
         // worth, is small against a solve), else the default tiling; "1" =
         // time them at any size; "0" = the default tensor-core tiling
         // everywhere; "alternate" = a fixed mix of tensor-core and CUDA-core
-        // depths, "bulk" = the bulk-copy variant everywhere (tests).
+        // depths (tests).
         const char* env = std::getenv("PSP_B200_SWEEP_AUTOTUNE");
         std::string mode = env ? env : "";
         if (mode.empty()) mode = h_.NumUnknowns() >= (int64_t(1) << 20) ? "1" : "0";
-        if (mode == "bulk") {  // the bulk-copy variant of the default tiling wherever there is one (tests)
-            for (ClassPlan& cp : P.cplan)
-                for (size_t d = 0; d < cp.fVar.size(); ++d) {
-                    auto firstBulk = [](const std::vector<SweepVariant>& vs) {
-                        for (size_t i = 0; i < vs.size(); ++i)
-                            if (vs[i].bulk) return (int)i;
-                        return 0;
-                    };
-                    cp.fSel[d] = firstBulk(cp.fVar[d]);
-                    cp.bSel[d] = firstBulk(cp.bVar[d]);
-                }
-        } else if (mode == "alternate") {
+        if (mode == "alternate") {
             for (ClassPlan& cp : P.cplan)
                 for (size_t d = 0; d < cp.fVar.size(); ++d) {
                     auto firstOf = [](const std::vector<SweepVariant>& vs, bool tc) {
@@ -1203,9 +1188,8 @@ bool FactorStore<R>::Autotune(SolvePlan& P) {
                         const std::vector<SweepVariant>& vs = (dir ? cp.bVar : cp.fVar)[d];
                         std::fprintf(stderr, dir ? "  bwd" : " fwd");
                         for (size_t i = 0; i < vs.size(); ++i)
-                            std::fprintf(stderr, " %s%s%d%s/%d %.4f", (int)i == (dir ? cp.bSel : cp.fSel)[d] ? "*" : "",
-                                         vs[i].tc ? "tc" : "cc", vs[i].cols, vs[i].bulk ? "b" : "", vs[i].chunk,
-                                         best[dir][d][i]);
+                            std::fprintf(stderr, " %s%s%d/%d %.4f", (int)i == (dir ? cp.bSel : cp.fSel)[d] ? "*" : "",
+                                         vs[i].tc ? "tc" : "cc", vs[i].cols, vs[i].chunk, best[dir][d][i]);
                     }
                     std::fprintf(stderr, "\n");
                 }
@@ -1261,7 +1245,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
         bool done = false;
         if constexpr (std::is_same<R, float>::value) {
             if (v.tc) {
-                LaunchSweepForwardTc(fr, tl, v.n, k, v.cols, v.bulk, w, st);
+                LaunchSweepForwardTc(fr, tl, v.n, k, v.cols, w, st);
                 done = true;
             }
         }
@@ -1281,7 +1265,7 @@ void FactorStore<R>::SolvePanel(z64* B, int ldk, int k, int p, int inMode, int o
         bool done = false;
         if constexpr (std::is_same<R, float>::value) {
             if (v.tc) {
-                LaunchSweepBackwardTc(fr, tl, v.n, B, k, v.cols, v.bulk, io, w, st);
+                LaunchSweepBackwardTc(fr, tl, v.n, B, k, v.cols, io, w, st);
                 done = true;
             }
         }

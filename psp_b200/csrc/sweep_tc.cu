@@ -86,13 +86,8 @@ constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 //   stage into a ring of RawSlots(fwd) slots shared by both groups (forward
 //   G's 128-row x 16-column box, [kc][row]; backward G^T's 128 x 16 box,
 //   [row][kc]); the forward keeps A in TMEM, so its last four slots reuse
-//   the A planes of the plane sets.  B comes one of two ways.  When a tile
-//   spans every right-hand side (k <= NC, k even) a stage's B rows are
-//   contiguous in global memory (forward [kc][plane][k], backward [kc][k])
-//   and the producer copies them with one bulk copy into B slot `slot`
-//   (the own-copy region, one per raw slot), completing on the same
-//   barrier as A; otherwise each group has a ring of kOwn slots of its own
-//   8-byte copies of B (forward [plane][kc][n], backward [kc][n]), every
+//   the A planes of the plane sets.  Each group has a ring of kOwn slots of
+//   its own copies of B (forward [plane][kc][n], backward [kc][n]), every
 //   entry read back by the thread that copied it.
 template <int NC>
 struct Cfg {
@@ -104,11 +99,11 @@ struct Cfg {
     static constexpr int kAccs = NC == 16 ? 4 : 2;
     static constexpr uint32_t kIdescHi = umma::InstrDescTf32(kTcRows, 4 * NC);
     static constexpr uint32_t kIdescLo = umma::InstrDescTf32(kTcRows, 2 * NC);
-    static constexpr int kAheadOwn = 2;                             // own stages in flight per group
+    static constexpr int kAheadOwn = NC == 16 ? 2 : 1;              // own stages in flight per group
     static constexpr int kOwn = kAheadOwn + 1;
-    __host__ __device__ static constexpr int RawSlots(bool fwd) { return NC == 16 ? 6 : 5; }
+    __host__ __device__ static constexpr int RawSlots(bool fwd) { return NC == 16 ? (fwd ? 8 : 6) : (fwd ? 7 : 5); }
     __host__ __device__ static constexpr int RawInRegion(bool fwd) {
-        return NC == 16 ? (fwd ? 2 : 6) : (fwd ? 1 : 5);
+        return NC == 16 ? (fwd ? 4 : 6) : (fwd ? 3 : 5);
     }
     __host__ __device__ static constexpr uint32_t OwnSlot(bool fwd) {
         return fwd ? 3 * kStageK * NC * 8 : kStageK * NC * 8;
@@ -127,8 +122,6 @@ struct Cfg {
     static_assert(RawSlots(true) - RawInRegion(true) == 2 * kPlaneSets && kRawA == kAPlane,
                   "the forward's extra raw slots are the plane sets' A planes");
     static_assert(RawSlots(true) <= kRawMax && RawSlots(false) <= kRawMax, "raw ring");
-    // bulk-copied B stages use the own-copy slots, one per raw slot
-    static_assert(RawSlots(true) <= kGroups * kOwn && RawSlots(false) <= kGroups * kOwn, "bulk B slots");
     static_assert(kAccs <= kAccMax && kOwn <= kOwnMax, "sync arrays");
     static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
     static_assert(kSmem <= 232448, "shared memory per CTA");
@@ -153,7 +146,7 @@ struct Sync {
     uint64_t accFull[kAccMax], accEmpty[kAccMax];
     uint64_t rawFull[kRawMax], rawEmpty[kRawMax];
     StageHdr hdr[kPlaneSets];
-    int rawInfo[kRawMax];        // stage place, packed (see InfoSt), written by the producer
+    int ownInfo[kGroups][kOwnMax];  // stage place, packed (see InfoSt); written and read by a group's first thread
     int rawK[kRawMax][2];        // stage's first K index and the tile's K end
     uint32_t tmem;
     int abort;
@@ -306,47 +299,19 @@ struct LoadCursor {
 // range are masked by the converters.
 template <int NC, bool kFwd>
 __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
-                             int k, int bulkB, unsigned char* smem, Sync& S, int* status) {
+                             int k, unsigned char* smem, Sync& S, int* status) {
     using C = Cfg<NC>;
     if ((threadIdx.x & 31) != 0) return;
-    unsigned char* bslots = smem + C::kRegionOff + C::OwnBase(kFwd);
-    const int rowEntries = kFwd ? 3 * k : k;  // complex entries of one B row
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
-    // Right-hand sides come from the preceding kernels: the B copies of the
-    // stages issued before that kernel has finished (the first ring's worth;
-    // their G copies go out at once) wait for it.
-    bool ready = !bulkB;
-    int pending = 0;
-    const c32* pendSrc[kRawMax];
-    uint32_t pendBytes[kRawMax];
-    auto flush = [&] {
-        PdlWait();
-        for (int i = 0; i < pending; ++i)
-            if (pendBytes[i]) umma::BulkCopy(bslots + i * C::OwnSlot(kFwd), pendSrc[i], pendBytes[i], &S.rawFull[i]);
-        ready = true;
-    };
     for (int g = 0; cur.Valid(g); ++g) {
         const int slot = g % C::RawSlots(kFwd);
-        if (!ready && g == C::RawSlots(kFwd)) flush();
         if (g >= C::RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / C::RawSlots(kFwd)) - 1) & 1, S, status)) return;
         const LoadMeta& m = cur.m;
         const int kBase = cur.KBase();
         S.rawK[slot][0] = kBase;
         S.rawK[slot][1] = m.ke;
-        S.rawInfo[slot] = cur.Info();
-        const int brows = bulkB ? max(0, min(kStageK, m.ke - kBase)) : 0;
-        const uint32_t bbytes = (uint32_t)brows * rowEntries * 8u;
-        umma::MbarArriveExpectTx(&S.rawFull[slot], kRawA + bbytes);
-        if (ready) {
-            if (bbytes)
-                umma::BulkCopy(bslots + slot * C::OwnSlot(kFwd), m.B + (int64_t)kBase * rowEntries, bbytes,
-                               &S.rawFull[slot]);
-        } else {  // g == slot here
-            pendSrc[pending] = m.B + (int64_t)kBase * rowEntries;
-            pendBytes[pending] = bbytes;
-            ++pending;
-        }
+        umma::MbarArriveExpectTx(&S.rawFull[slot], kRawA);
         const unsigned char* map = reinterpret_cast<const unsigned char*>(m.tmap) + (kFwd ? 0 : 128);
         if (kFwd)
             umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, m.row0, kBase, &S.rawFull[slot]);
@@ -354,7 +319,6 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
             umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, kBase, m.row0, &S.rawFull[slot]);
         cur.Advance();
     }
-    if (!ready) flush();
 }
 
 // ------------------------------------------------------------------ converters
@@ -370,14 +334,8 @@ __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
 // the tile), commits one copy group and moves the cursor to the group's
 // next stage.
 template <int NC, bool kFwd>
-__device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* own, int bulkB) {
+__device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* own, int gr, Sync& S) {
     using C = Cfg<NC>;
-    if (bulkB) {  // B arrives with A: only walk the stages
-        if (cur.total < 0)
-#pragma unroll
-            for (int i = 0; i < kGroups; ++i) cur.Advance();
-        return;
-    }
     if (cur.total >= 0) {
         umma::CpAsyncCommit();
         return;
@@ -385,6 +343,7 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
     const int slot = (cur.gl / kGroups) % C::kOwn;
     const LoadMeta& m = cur.m;
     const int ct = (threadIdx.x - kLoad0) % kGroupThreads;
+    if (ct == 0) S.ownInfo[gr][slot] = cur.Info();
     unsigned char* base = own + slot * C::OwnSlot(kFwd);
     c32* rb = reinterpret_cast<c32*>(base);
     const int ncol = min(NC, cur.k - m.col0);
@@ -413,7 +372,7 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
 // K-columns at or beyond kValid are taken as zero.
 template <int NC, bool kFwd>
 __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned char* rawA, const unsigned char* own,
-                                             int kValid, int ct, uint32_t tmemA, int bulkB, int k) {
+                                             int kValid, int ct, uint32_t tmemA) {
     using C = Cfg<NC>;
     unsigned char* aHi = P;
     unsigned char* aLo = P + kAPlane;
@@ -458,14 +417,7 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
     for (int j = 0; j < kStageK * NC / kGroupThreads; ++j) {
         const int e = ct + j * kGroupThreads;
         const int kc = e / NC, nn = e % NC;
-        c32 b;
-        if (bulkB) {  // rows [kc][plane][k] (forward) or [kc][k]; rows past kValid are stale
-            const c32* row = rb + kc * (kFwd ? 3 * k : k);
-            const bool ok = kc < kValid && nn < k;
-            b = ok ? (kFwd ? row[nn] + row[k + nn] + row[2 * k + nn] : row[nn]) : zero;
-        } else {
-            b = kFwd ? rb[e] + rb[kStageK * NC + e] + rb[2 * kStageK * NC + e] : rb[e];
-        }
+        const c32 b = kFwd ? rb[e] + rb[kStageK * NC + e] + rb[2 * kStageK * NC + e] : rb[e];
         float2 h, l;
         Split2(b, h, l);
         const uint32_t o0 = umma::Sw128Offset(2 * nn, kc >> 1) + (kc & 1) * 8;
@@ -481,19 +433,17 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
 // ends the stream; false when the role is done.
 template <int NC, bool kFwd>
 __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char* own, const LoadCursor<kFwd>& cur,
-                                              int g, int gr, int ct, int bulkB, int k, Sync& S, int* status) {
+                                              int g, int gr, int ct, Sync& S, int* status) {
     using C = Cfg<NC>;
     const int ps = gr, slot = g % C::RawSlots(kFwd), oslot = (g / kGroups) % C::kOwn;
     const bool valid = cur.Valid(g);
     if (valid && !Wait(&S.rawFull[slot], (g / C::RawSlots(kFwd)) & 1, S, status)) return false;
     if (g >= kGroups && !Wait(&S.planeEmpty[ps], ((g / kGroups) - 1) & 1, S, status)) return false;
-    if (!bulkB) umma::CpAsyncWait<C::kAheadOwn>();  // this thread's own copies of stage g have landed
+    umma::CpAsyncWait<C::kAheadOwn>();  // this thread's own copies of stage g have landed
     if (valid) {
         const int kValid = S.rawK[slot][1] - S.rawK[slot][0];
-        const unsigned char* bsrc = bulkB ? smem + C::kRegionOff + C::OwnBase(kFwd) + slot * C::OwnSlot(kFwd)
-                                          : own + oslot * C::OwnSlot(kFwd);
-        ConvertStage<NC, kFwd>(smem + ps * C::kPlaneSet, RawSlotPtr<NC, kFwd>(smem, slot), bsrc, kValid, ct,
-                               S.tmem + C::ACol(ps), bulkB, k);
+        ConvertStage<NC, kFwd>(smem + ps * C::kPlaneSet, RawSlotPtr<NC, kFwd>(smem, slot),
+                               own + oslot * C::OwnSlot(kFwd), kValid, ct, S.tmem + C::ACol(ps));
     }
     if (kFwd) {
         umma::TmemStoreWait();
@@ -501,7 +451,7 @@ __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char
     }
     umma::FenceProxyAsync();
     if (ct == 0) {
-        const int info = valid ? S.rawInfo[slot] : 0;
+        const int info = S.ownInfo[gr][oslot];
         S.hdr[ps] = valid ? StageHdr{1, InfoSt(info), InfoNst(info), InfoJ(info)} : StageHdr{0, 0, 0, 0};
     }
     umma::MbarArrive(&S.planeFull[ps]);
@@ -511,7 +461,7 @@ __device__ __forceinline__ bool ConverterStep(unsigned char* smem, unsigned char
 
 template <int NC, bool kFwd>
 __device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const SweepTile* __restrict__ tiles, int n,
-                              int k, int bulkB, unsigned char* smem, Sync& S, int* status) {
+                              int k, unsigned char* smem, Sync& S, int* status) {
     using C = Cfg<NC>;
     const int lt = threadIdx.x - kLoad0;
     const int gr = lt / kGroupThreads, ct = lt % kGroupThreads;
@@ -521,10 +471,10 @@ __device__ void ConverterRole(const SweepFront<float>* __restrict__ fr, const Sw
     for (int i = 0; i < gr; ++i) cur.Advance();
     PdlWait();  // right-hand sides come from the preceding kernels
 #pragma unroll
-    for (int a = 0; a < C::kAheadOwn; ++a) IssueOwn<NC>(cur, own, bulkB);
+    for (int a = 0; a < C::kAheadOwn; ++a) IssueOwn<NC>(cur, own, gr, S);
     for (int g = gr;; g += kGroups) {
-        IssueOwn<NC>(cur, own, bulkB);
-        if (!ConverterStep<NC, kFwd>(smem, own, cur, g, gr, ct, bulkB, k, S, status)) break;
+        IssueOwn<NC>(cur, own, gr, S);
+        if (!ConverterStep<NC, kFwd>(smem, own, cur, g, gr, ct, S, status)) break;
     }
     umma::CpAsyncWaitAll();
 }
@@ -786,7 +736,7 @@ __device__ __forceinline__ unsigned char* SmemBase() {
 template <int NC>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const SweepFront<float>* __restrict__ fr,
                                                                          const SweepTile* __restrict__ tiles, int n,
-                                                                         int k, int bulkB, SweepWork work) {
+                                                                         int k, SweepWork work) {
     __shared__ Sync S;
     unsigned char* smem = SmemBase();
     PdlTrigger();
@@ -796,11 +746,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
         EpilogueRole<NC, true>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + Cfg<NC>::kStagingOff), S,
                                nullptr, PanelIO{});
     } else if (tid < kMma0) {
-        ConverterRole<NC, true>(fr, tiles, n, k, bulkB, smem, S, work.status);
+        ConverterRole<NC, true>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
         MmaRole<NC, true>(smem, S, work.status);
     } else if (tid >= kProd0) {
-        ProducerRole<NC, true>(fr, tiles, n, k, bulkB, smem, S, work.status);
+        ProducerRole<NC, true>(fr, tiles, n, k, smem, S, work.status);
     }
     Teardown(S);
 }
@@ -808,8 +758,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
 template <int NC>
 __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const SweepFront<float>* __restrict__ fr,
                                                                           const SweepTile* __restrict__ tiles, int n,
-                                                                          z64* __restrict__ B, int k, int bulkB,
-                                                                          PanelIO io, SweepWork work) {
+                                                                          z64* __restrict__ B, int k, PanelIO io,
+                                                                          SweepWork work) {
     __shared__ Sync S;
     unsigned char* smem = SmemBase();
     PdlTrigger();
@@ -819,11 +769,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const 
         EpilogueRole<NC, false>(fr, tiles, n, k, work, reinterpret_cast<c32*>(smem + Cfg<NC>::kStagingOff), S, B,
                                 io);
     } else if (tid < kMma0) {
-        ConverterRole<NC, false>(fr, tiles, n, k, bulkB, smem, S, work.status);
+        ConverterRole<NC, false>(fr, tiles, n, k, smem, S, work.status);
     } else if (tid == kMma0) {
         MmaRole<NC, false>(smem, S, work.status);
     } else if (tid >= kProd0) {
-        ProducerRole<NC, false>(fr, tiles, n, k, bulkB, smem, S, work.status);
+        ProducerRole<NC, false>(fr, tiles, n, k, smem, S, work.status);
     }
     Teardown(S);
 }
@@ -876,31 +826,27 @@ void PrepareSweepTcKernels() {
                                     (int)Cfg<32>::kSmem));
 }
 
-bool SweepTcBulkB(int k, int cols) { return k <= cols && k % 2 == 0; }
-
-void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols, bool bulk,
+void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols,
                           const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    const int bulkB = bulk && SweepTcBulkB(k, cols) ? 1 : 0;
     if (cols == 32)
         LaunchPdl(sweep_tc_forward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles, n,
-                  k, bulkB, w);
+                  k, w);
     else
         LaunchPdl(sweep_tc_forward_kernel<16>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<16>::kSmem, st, fr, tiles, n,
-                  k, bulkB, w);
+                  k, w);
     CUDA_LAUNCH_CHECK();
 }
 
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k, int cols,
-                           bool bulk, const PanelIO& io, const SweepWork& w, cudaStream_t st) {
+                           const PanelIO& io, const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
-    const int bulkB = bulk && SweepTcBulkB(k, cols) ? 1 : 0;
     if (cols == 32)
         LaunchPdl(sweep_tc_backward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles,
-                  n, B, k, bulkB, io, w);
+                  n, B, k, io, w);
     else
         LaunchPdl(sweep_tc_backward_kernel<16>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<16>::kSmem, st, fr, tiles,
-                  n, B, k, bulkB, io, w);
+                  n, B, k, io, w);
     CUDA_LAUNCH_CHECK();
 }
 

@@ -95,20 +95,17 @@ def test_mixed_route_solve_converges(setup):
 
 @pytest.mark.parametrize("k", [16, 32, 40])
 def test_wide_tensor_core_tiles_match(product_lib, k):
-    """Tile widths and right-hand-side copies of the tensor-core kernels:
-    more than 16 right-hand sides take 32-wide tiles (each G stage split
-    once for all of them); when a tile spans every right-hand side (k = 16,
-    32) a stage's right-hand-side rows arrive by one bulk copy with the G
-    stage, otherwise (k = 40: a full and a partly filled tile) by per-thread
-    copies; the small fronts' short K-chunks exercise the split-K reduction
-    per 16-column sub-tile.  The preconditioner and every panel solve agree
-    with the CUDA-core kernels and the oracle, and a mixed solve converges
-    like the oracle's."""
+    """Tile widths of the tensor-core kernels: more than 16 right-hand sides
+    take 32-wide tiles (each G stage split once for all of them; k = 40
+    leaves a partly filled last tile), 16 take 16-wide ones; the small
+    fronts' short K-chunks exercise the split-K reduction per 16-column
+    sub-tile.  The preconditioner and every panel solve agree with the
+    CUDA-core kernels and the oracle, and a mixed solve converges like the
+    oracle's."""
     w = W.small_case(**dict(CASE, k=k))
     O = oracle_for(w.disc)
     O.initialize(w.velocity)
-    mode = "bulk" if k in (16, 32) else "0"
-    wide = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": mode, "PSP_B200_SWEEP_CUDA_CORES": None})
+    wide = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": "0", "PSP_B200_SWEEP_CUDA_CORES": None})
     cc = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": None, "PSP_B200_SWEEP_CUDA_CORES": "1"})
     ref = O.precondition(w.rhs)
     x = wide.precondition(w.rhs)
