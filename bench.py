@@ -50,7 +50,7 @@ RESTART = 20
 # CPU model multiplies its sampled per-step costs by this count (the FP64 GPU
 # path runs the oracle's algorithm step for step, so its count is the
 # oracle's).  Workloads not listed use the count of the run's own solve.
-FP64_ITERATIONS = {"smooth_anomalies_116": 15, "plain_bump_50": 16}
+FP64_ITERATIONS = {"smooth_anomalies_116": 15, "plain_bump_50": 16, "large_220": 8}
 
 
 def parse():
@@ -697,6 +697,10 @@ def main():
             "data": "synthetic", "config": config_dict(args.config, w, kb),
             "setup_ms": 1e3 * setup_s, "setup_plus_solve_rhs_per_s": setup_plus_solve,
             "iterations": st_m["iterations"], "final_rel_resid": st_m["final_max_rel_resid"],
+            # device time of the last timed Solve by phase (events at GMRES's own sync points)
+            "solve_phases_s": {"precondition": st_m["precondition_seconds"], "matvec": st_m["matvec_seconds"],
+                               "arnoldi": st_m["arnoldi_seconds"], "preconditions": st_m["num_preconditions"],
+                               "wall": st_m["solve_seconds"]},
             "converged": all(s["converged"] for s in mixed["stats"]),
             "memory": mem_mixed,
             "fp64": fp64,

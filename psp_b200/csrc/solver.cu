@@ -920,9 +920,16 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // nothing extra and save split-K partial sums) and only shrinks to give
     // every SM tiles; `forceChunk` > 0 fixes it instead (tuning candidates).
     int64_t maxPartialRows = kTcRows, maxCounters = 1;
+    // Longest K-chunk of a tensor-core tile (PSP_B200_SWEEP_TC_MAX_CHUNK, a
+    // power of two from 16 to 512), and a fixed chunk for the default
+    // tensor-core tiling in place of the shrinking rule below
+    // (PSP_B200_SWEEP_TC_CHUNK, tests).
+    const int tcMaxChunk = (int)std::max(16LL, std::min(512LL, EnvInt("PSP_B200_SWEEP_TC_MAX_CHUNK", 512)));
+    const int tcFixedChunk = (int)std::max(0LL, std::min((long long)tcMaxChunk, EnvInt("PSP_B200_SWEEP_TC_CHUNK", 0)));
     auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, bool tcTiles, int cols, int forceChunk,
                          std::vector<SweepTile>& tiles) {
-        const int maxChunk = tcTiles ? 512 : SweepMaxChunk<R>();
+        const int maxChunk = tcTiles ? tcMaxChunk : SweepMaxChunk<R>();
+        if (forceChunk > maxChunk) forceChunk = maxChunk;
         const int tileRows = tcTiles ? kTcRows : kSweepRows;
         const int subs = cols / kSweepCols;  // partial slots and counters per split tile
         auto build = [&](int kc, bool emit) {
@@ -989,7 +996,7 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
         std::vector<Cand> cand;
         if (tc_) {
             const int wide = k > kSweepCols ? 32 : kSweepCols;
-            cand.push_back({true, wide, 0});
+            cand.push_back({true, wide, tcFixedChunk});
             for (int kc : {64, 128, 256, 512}) cand.push_back({true, wide, kc});
             if (wide != kSweepCols)
                 for (int kc : {0, 512}) cand.push_back({true, kSweepCols, kc});

@@ -30,12 +30,13 @@
 //                       copies its own right-hand-side entries kAhead
 //                       stages ahead
 //   MMA (1 thread)      tcgen05.mma per stage into one of kAccs TMEM
-//                       accumulators (round robin by tile)
-//   epilogue (4 warps)  TMEM -> registers, split-K reduction, and the result
-//                       through shared memory so that its global accesses
-//                       are coalesced; meanwhile it sets up the accumulator
-//                       of the tile kAccs ahead, so its global latency never
-//                       holds up the tensor core.
+//                       accumulators (round robin by chain: a tile's stages
+//                       in runs of kChainStages)
+//   epilogue (4 warps)  TMEM -> registers: the chains of a tile summed in
+//                       FP32, split-K reduction, and the result through
+//                       shared memory so that its global accesses are
+//                       coalesced; what the write-out reads from global
+//                       memory is loaded before the accumulator is ready.
 // Every wait on an mbarrier is bounded; a timeout sets bit 2 of the status
 // word and a shared abort flag that ends every role's loop; the CTA then
 // frees tensor memory and returns, leaving unfinished tiles unwritten.
@@ -70,6 +71,14 @@ constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kRawA = kStageK * kTcRows * 8;      // 16 KB
 constexpr int kRawMax = 8;
 constexpr int kAccMax = 4, kOwnMax = 3;
+// The tensor core adds each MMA's products into its FP32 accumulator with
+// truncation, so long accumulation chains in TMEM lose accuracy (a K-chunk of
+// 512 columns left the large layered model's preconditioner 9e-5 away from
+// FP32 CUDA-core arithmetic, and GMRES took 21 steps instead of 9).  Each
+// accumulator therefore holds at most kChainStages stages (64 complex K);
+// the epilogue sums the chains of a tile in FP32 (round to nearest) into a
+// TMEM sum region, and adds the last chain on the way out.
+constexpr int kChainStages = 4;
 
 // The result passes through shared memory 16 right-hand sides (one sub-tile)
 // at a time, with row stride kOutPad.
@@ -119,11 +128,13 @@ struct Cfg {
     __host__ __device__ static constexpr uint32_t ACol(int ps) {
         return kAccs * kAccCols + (uint32_t)ps * 2 * kAStageCols;
     }
+    // the running sum of a tile's finished chains: NC complex per lane
+    static constexpr uint32_t kSumCol = kAccs * kAccCols + kPlaneSets * 2 * kAStageCols;
     static_assert(RawSlots(true) - RawInRegion(true) == 2 * kPlaneSets && kRawA == kAPlane,
                   "the forward's extra raw slots are the plane sets' A planes");
     static_assert(RawSlots(true) <= kRawMax && RawSlots(false) <= kRawMax, "raw ring");
     static_assert(kAccs <= kAccMax && kOwn <= kOwnMax, "sync arrays");
-    static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
+    static_assert(kSumCol + 2 * NC <= kTmemCols, "accumulators, A stages and the chain sum fit in TMEM");
     static_assert(kSmem <= 232448, "shared memory per CTA");
 };
 
@@ -502,20 +513,31 @@ __device__ __forceinline__ void IssueStage(const unsigned char* P, uint32_t tmem
     }
 }
 
+// A tile's stages form chains of kChainStages; chain q (counted over the
+// CTA's tiles) accumulates in accumulator q % kAccs.
+__device__ __forceinline__ bool ChainFirst(int st) { return st % kChainStages == 0; }
+__device__ __forceinline__ bool ChainLast(int st, int nst) { return st % kChainStages == kChainStages - 1 || st == nst - 1; }
+__device__ __forceinline__ int NumChains(int nst) { return (nst + kChainStages - 1) / kChainStages; }
+
 template <int NC, bool kFwd>
 __device__ void MmaRole(const unsigned char* planes, Sync& S, int* status) {
     using C = Cfg<NC>;
+    int q = 0;  // chains finished
     for (int g = 0;; ++g) {
         const int ps = g % kPlaneSets;
         if (!Wait(&S.planeFull[ps], (g / kPlaneSets) & 1, S, status)) return;
         const StageHdr h = S.hdr[ps];
         if (!h.valid) return;  // the epilogue counts its own tiles
-        const int b = h.j % C::kAccs;
-        if (h.st == 0 && !Wait(&S.accEmpty[b], (h.j / C::kAccs) & 1, S, status)) return;
+        const int b = q % C::kAccs;
+        const bool first = ChainFirst(h.st);
+        if (first && !Wait(&S.accEmpty[b], (q / C::kAccs) & 1, S, status)) return;
         umma::FenceAfterSync();
-        IssueStage<NC, kFwd>(planes + ps * C::kPlaneSet, S.tmem + b * C::kAccCols, S.tmem + C::ACol(ps), h.st > 0);
+        IssueStage<NC, kFwd>(planes + ps * C::kPlaneSet, S.tmem + b * C::kAccCols, S.tmem + C::ACol(ps), !first);
         umma::CommitTo(&S.planeEmpty[ps]);
-        if (h.st == h.nst - 1) umma::CommitTo(&S.accFull[b]);
+        if (ChainLast(h.st, h.nst)) {
+            umma::CommitTo(&S.accFull[b]);
+            ++q;
+        }
     }
 }
 
@@ -624,6 +646,27 @@ __device__ __forceinline__ void LoadAccumulator(uint32_t taddr, int h, c32 (&acc
     }
 }
 
+// Sub-tile h of a tile's chain sum (TMEM address tsum of this warp's lanes,
+// 16 complex columns at 32 h): acc += sum, or sum := acc.
+__device__ __forceinline__ void AddSum(uint32_t tsum, int h, c32 (&acc)[kSweepCols]) {
+    float v[kSweepCols];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        umma::TmemLoad16(tsum + 2 * kSweepCols * h + kSweepCols * q, v);
+#pragma unroll
+        for (int c = 0; c < kSweepCols / 2; ++c) acc[8 * q + c] += mk(v[2 * c], v[2 * c + 1]);
+    }
+}
+__device__ __forceinline__ void StoreSum(uint32_t tsum, int h, const c32 (&acc)[kSweepCols]) {
+    float v[2 * kSweepCols];
+#pragma unroll
+    for (int c = 0; c < kSweepCols; ++c) {
+        v[2 * c] = acc[c].re;
+        v[2 * c + 1] = acc[c].im;
+    }
+    umma::TmemStore32NoWait(tsum + 2 * kSweepCols * h, v);
+}
+
 // Coalesced write-out of a sub-tile from the staging tile.
 template <bool kFwd>
 __device__ __forceinline__ void StoreTile(const SweepFront<float>& f, const SweepTile& t, int k, int coff,
@@ -663,22 +706,49 @@ __device__ void EpilogueRole(const SweepFront<float>* __restrict__ fr, const Swe
     int ti;
     PdlWait();  // carries, split-K scratch and outputs are shared with the preceding kernels
     for (int q = 0; q < C::kAccs; ++q) umma::MbarArrive(&S.accEmpty[q]);  // every accumulator starts free
+    const uint32_t lanes = (uint32_t)(warp * 32) << 16;
+    const uint32_t tsum = S.tmem + C::kSumCol + lanes;
+    int q = 0;  // chains drained
     for (int j = 0; TileOf(tiles, n, j, ti); ++j) {
-        const int b = j % C::kAccs;
         const SweepTile t = tiles[ti];
         const SweepFront<float> f = fr[t.front];
+        int kb, ke, nst;
+        TileRange(t, kFwd, kb, ke, nst);
+        const int nch = NumChains(nst);
+        // every chain but the last goes into the sum region; every epilogue
+        // thread takes the same branches (they share named barriers)
+        for (int c = 0; c + 1 < nch; ++c, ++q) {
+            const int b = q % C::kAccs;
+            const bool ok = Wait(&S.accFull[b], (q / C::kAccs) & 1, S, w.status);
+            if (umma::NamedBarrierOr(1, kEpiThreads, !ok)) return;
+            umma::FenceAfterSync();
+            const uint32_t taddr = S.tmem + b * C::kAccCols + lanes;
+#pragma unroll 1
+            for (int h = 0; h < C::kSubs; ++h) {
+                c32 acc[kSweepCols];
+                LoadAccumulator<NC>(taddr, h, acc);
+                if (c > 0) AddSum(tsum, h, acc);
+                StoreSum(tsum, h, acc);
+            }
+            umma::TmemStoreWait();
+            umma::FenceBeforeSync();
+            umma::MbarArrive(&S.accEmpty[b]);
+        }
+        // the write-out's global reads overlap the last chain's MMAs
         SubPrefetch pf;
         PrefetchSub<kFwd>(f, t, k, 0, io, pf);
-        // every epilogue thread takes the same branch (they share named barriers)
-        const bool ok = Wait(&S.accFull[b], (j / C::kAccs) & 1, S, w.status);
+        const int b = q % C::kAccs;
+        const bool ok = Wait(&S.accFull[b], (q / C::kAccs) & 1, S, w.status);
+        ++q;
         if (umma::NamedBarrierOr(1, kEpiThreads, !ok)) return;
         umma::FenceAfterSync();
-        const uint32_t taddr = S.tmem + b * C::kAccCols + ((uint32_t)(warp * 32) << 16);
+        const uint32_t taddr = S.tmem + b * C::kAccCols + lanes;
 #pragma unroll
         for (int h = 0; h < C::kSubs; ++h) {
             if (h > 0) PrefetchSub<kFwd>(f, t, k, h * kSweepCols, io, pf);
             c32 acc[kSweepCols];
             LoadAccumulator<NC>(taddr, h, acc);
+            if (nch > 1) AddSum(tsum, h, acc);
             if (h == C::kSubs - 1) {
                 umma::FenceBeforeSync();
                 umma::MbarArrive(&S.accEmpty[b]);
