@@ -126,10 +126,10 @@ def test_long_chunks_sum_their_chains_in_fp32(product_lib):
     complex K) in one TMEM accumulator and the epilogue sums these chains in
     FP32.  A tiling of 512-column K-chunks (chains summed inside the tile)
     and one of 64-column chunks (one chain per tile, the chunks summed by the
-    split-K reduction in the same order) must give the same preconditioner;
-    both agree with the CUDA-core kernels and the oracle.  The root fronts
-    here have K ranges of several hundred columns, so the long tiles hold up
-    to eight chains."""
+    split-K reduction) run the same MMAs per chain and must agree to FP32
+    rounding (a lost or repeated chain would be off by O(1)); both agree with
+    the CUDA-core kernels and the oracle.  The root fronts here have K ranges
+    of several hundred columns, so the long tiles hold up to eight chains."""
     w = W.small_case(**dict(CASE, k=32))
     O = oracle_for(w.disc)
     O.initialize(w.velocity)
@@ -138,8 +138,8 @@ def test_long_chunks_sum_their_chains_in_fp32(product_lib):
     short = _mixed_handle(w, dict(env, PSP_B200_SWEEP_TC_CHUNK="64"))
     cc = _mixed_handle(w, {"PSP_B200_SWEEP_AUTOTUNE": None, "PSP_B200_SWEEP_CUDA_CORES": "1"})
     x_long, x_short = long_.precondition(w.rhs), short.precondition(w.rhs)
-    assert rel(x_long, x_short) < 1e-9
+    assert rel(x_long, x_short) < 1e-6
     assert rel(x_long, cc.precondition(w.rhs)) < 2e-5
     assert rel(x_long, O.precondition(w.rhs)) < 1e-4
     for p in range(O.geometry().shape[0]):
-        assert rel(long_.solve_panel(w.rhs, p), short.solve_panel(w.rhs, p)) < 1e-9, p
+        assert rel(long_.solve_panel(w.rhs, p), short.solve_panel(w.rhs, p)) < 1e-6, p
