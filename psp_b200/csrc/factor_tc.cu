@@ -62,11 +62,18 @@ constexpr uint32_t kStageOff = kRawOff + kRaw * kRawSlot;  // C staging [col][ro
 constexpr size_t kFactorTcSmem = kStageOff + (size_t)kBN * kBM * 8 + 1024;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kIdesc = umma::InstrDescTf32(kBM, 2 * kBN);
-constexpr int kFirst = 1, kLast = 2;  // stage flags
+constexpr int kFirst = 1, kLast = 2;  // stage flags: a tile's first and last stage
+// The tensor core adds each MMA's products into its FP32 accumulator with
+// truncation, so an accumulator holds at most kChainStages stages (64
+// complex K); the epilogue sums a tile's chains in FP32 (round to nearest)
+// in a TMEM sum region and adds the last chain on the way out.
+constexpr int kChainStages = 8;
+constexpr int kChainFirst = 4, kChainLast = 8;  // stage flags: a chain's first and last stage
+constexpr uint32_t kSumCol = ACol(kPlaneSets);   // 2 kBN columns
 
 static_assert(kRawSlot % 16 == 0 && kStageOff % 16 == 0, "copy targets stay 16-byte aligned");
 static_assert(kPlSet % 1024 == 0 && kBPl % 512 == 0, "swizzle atoms stay aligned");
-static_assert(ACol(kPlaneSets) <= kTmemCols, "accumulators and A stages fit in TMEM");
+static_assert(kSumCol + kAccCols <= kTmemCols, "accumulators, A stages and the chain sum fit in TMEM");
 static_assert(kFactorTcSmem <= 232448, "shared memory per CTA");
 static_assert(kConvThreads == 2 * kBM && kConvThreads == 4 * kBN, "converter thread mapping");
 
@@ -218,7 +225,10 @@ __device__ void ConverterRole(const GemmTcTile* tiles, int n, unsigned char* sme
         if (more) {
             const int slot = issued % kRaw;
             IssueStage(cur, st, raw + slot * kRawSlot, ct);
-            if (ct == 0) S.rawFlags[slot] = (st == 0 ? kFirst : 0) | (st == nst - 1 ? kLast : 0);
+            if (ct == 0)
+                S.rawFlags[slot] = (st == 0 ? kFirst : 0) | (st == nst - 1 ? kLast : 0) |
+                                   (st % kChainStages == 0 ? kChainFirst : 0) |
+                                   (st % kChainStages == kChainStages - 1 || st == nst - 1 ? kChainLast : 0);
             ++issued;
             if (++st == nst) {
                 t += G;
@@ -259,13 +269,13 @@ __device__ void ConverterRole(const GemmTcTile* tiles, int n, unsigned char* sme
 __device__ void MmaRole(int n, unsigned char* smem, Sync& S, int* status) {
     const int G = gridDim.x;
     const int ntiles = (int)blockIdx.x < n ? (n - (int)blockIdx.x + G - 1) / G : 0;
-    int g = 0;
+    int g = 0, q = 0;  // stages and chains issued
     for (int i = 0; i < ntiles; ++g) {
-        const int p = g % kPlaneSets, a = i % kAccs;
+        const int p = g % kPlaneSets, a = q % kAccs;
         if (!Wait(&S.planeFull[p], (g / kPlaneSets) & 1, S, status)) return;
         const int flags = *reinterpret_cast<volatile int*>(&S.planeFlags[p]);
-        const bool first = flags & kFirst;
-        if (first && i >= kAccs && !Wait(&S.accEmpty[a], ((i / kAccs) - 1) & 1, S, status)) return;
+        const bool first = flags & kChainFirst;
+        if (first && q >= kAccs && !Wait(&S.accEmpty[a], ((q / kAccs) - 1) & 1, S, status)) return;
         umma::FenceAfterSync();
         const uint32_t acc = S.tmem + a * kAccCols, aHi = S.tmem + ACol(p), aLo = aHi + kACols;
         const uint32_t bHi = umma::SmemAddr(smem + p * kPlSet), bLo = bHi + kBPl;
@@ -277,10 +287,11 @@ __device__ void MmaRole(int n, unsigned char* smem, Sync& S, int* status) {
             umma::MmaTf32TmemA(acc, aLo + 8 * s, bh, kIdesc, 1u);
         }
         umma::CommitTo(&S.planeEmpty[p]);
-        if (flags & kLast) {
+        if (flags & kChainLast) {
             umma::CommitTo(&S.accFull[a]);
-            ++i;
+            ++q;
         }
+        if (flags & kLast) ++i;
     }
 }
 
@@ -326,12 +337,42 @@ __device__ void EpilogueRole(const GemmTcTile* tiles, int n, c32* stage, Sync& S
         IssueC(cur, stage);
     }
     umma::CpAsyncCommit();
-    int i = 0;
-    for (int t = blockIdx.x; t < n; t += G, ++i) {
-        const int a = i % kAccs;
+    const uint32_t tsum = S.tmem + lane + kSumCol;
+    int q = 0;  // chains drained
+    for (int t = blockIdx.x; t < n; t += G) {
         GemmTcTile nxt;
         if (t + G < n) nxt = tiles[t + G];
-        const bool ok = Wait(&S.accFull[a], (i / kAccs) & 1, S, status);
+        // every chain but the last goes into the sum region; every epilogue
+        // thread takes the same branches (they share named barriers)
+        const int nch = (StagesOf(cur) + kChainStages - 1) / kChainStages;
+        bool quit = false;  // the same on every epilogue thread
+        for (int c = 0; c + 1 < nch && !quit; ++c, ++q) {
+            const int a = q % kAccs;
+            const bool ok = Wait(&S.accFull[a], (q / kAccs) & 1, S, status);
+            quit = umma::NamedBarrierOr(2, kEpiThreads, !ok);
+            if (quit) break;
+            umma::FenceAfterSync();
+            const uint32_t acc = S.tmem + lane + a * kAccCols;
+#pragma unroll 1
+            for (int j = 0; j < kBN / 16; ++j) {
+                float v[32];
+                umma::TmemLoad32(acc + 32 * j, v);
+                if (c > 0) {
+                    float w[32];
+                    umma::TmemLoad32(tsum + 32 * j, w);
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) v[e] += w[e];
+                }
+                umma::TmemStore32NoWait(tsum + 32 * j, v);
+            }
+            umma::TmemStoreWait();
+            umma::FenceBeforeSync();
+            umma::MbarArrive(&S.accEmpty[a]);
+        }
+        if (quit) break;
+        const int a = q % kAccs;
+        const bool ok = Wait(&S.accFull[a], (q / kAccs) & 1, S, status);
+        ++q;
         umma::CpAsyncWaitAll();
         if (umma::NamedBarrierOr(2, kEpiThreads, !ok)) break;  // the staged C is visible
         umma::FenceAfterSync();
@@ -341,6 +382,12 @@ __device__ void EpilogueRole(const GemmTcTile* tiles, int n, c32* stage, Sync& S
         for (int j = 0; j < kBN / 16; ++j) {
             float v[32];
             umma::TmemLoad32(acc + 32 * j, v);
+            if (nch > 1) {
+                float w[32];
+                umma::TmemLoad32(tsum + 32 * j, w);
+#pragma unroll
+                for (int e = 0; e < 32; ++e) v[e] += w[e];
+            }
             if (full)
                 StoreCols<true>(cur, v, stage, 16 * j);
             else
