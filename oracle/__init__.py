@@ -115,6 +115,16 @@ class Oracle:
         lib().oracle_geometry(self._h, ctypes.byref(n), _ptr(info, ctypes.c_int))
         return info.reshape(n.value, 4)  # (vLow, depth, padding, class)
 
+    def stretch(self, which, idx, v_offset=0):
+        """PML stretch `which` (1 s1Inv, 2 s2Inv, 3 s3Inv, 4 s3InvArtificial
+        with v_offset) at the indices idx, complex128."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        out = np.zeros(idx.size, dtype=np.complex128)
+        lib().oracle_stretch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        lib().oracle_stretch(self._h, which, idx.size, _ptr(idx, ctypes.c_int), v_offset, _ptr(out.view(np.float64)))
+        return out
+
     def nd_to_natural(self):
         out = np.zeros(self.N, dtype=np.int32)
         lib().oracle_nd_to_natural(self._h, _ptr(out, ctypes.c_int))

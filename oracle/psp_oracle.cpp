@@ -809,6 +809,21 @@ int oracle_create(const oracle_disc* d, double damping, int planesPerPanel, int 
 void oracle_destroy(void* h) { delete (Solver*)h; }
 
 // Geometry summary: numPanels, then per panel (vLow, depth, padding, class).
+// PML stretch `which` (1 s1Inv, 2 s2Inv, 3 s3Inv, 4 s3InvArtificial with
+// vOffset) at n indices, as (re, im) pairs.
+int oracle_stretch(void* h, int which, int n, const int* idx, int vOffset, double* out) {
+    const Solver& S = *(const Solver*)h;
+    for (int i = 0; i < n; ++i) {
+        const C c = which == 1 ? s1Inv(S, idx[i])
+                  : which == 2 ? s2Inv(S, idx[i])
+                  : which == 3 ? s3Inv(S, idx[i])
+                               : s3InvArtificial(S, idx[i], vOffset);
+        out[2 * i] = c.real();
+        out[2 * i + 1] = c.imag();
+    }
+    return 0;
+}
+
 int oracle_geometry(void* h, int* numPanels, int* panelInfo) {
     Solver& S = *(Solver*)h;
     *numPanels = S.numPanels;

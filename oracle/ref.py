@@ -88,3 +88,113 @@ def write_volume(grid, basename):
     g, c = _in(grid)
     nz, ny, nx, ns = g.shape
     _check(lib().ref_grid_write_volume(_dp(g), nx, ny, nz, ns, c, os.fsencode(basename)))
+
+
+class RefHelmholtz:
+    """The reference's own psp::DistHelmholtz<double> on one process, built
+    by its constructor (geometry, nested-dissection ordering and elimination
+    trees; Clique's symbolic analysis is not reproduced), for the members
+    that need no frontal structure: PanelV / PanelDepth / PanelPadding, the
+    global row order, the PML stretches and the global rows Initialize
+    forms.  ``disc`` is a psp_b200 Discretization."""
+
+    def __init__(self, disc, damping=7.0, planes_per_panel=4, cutoff=12):
+        L = lib()
+        L.ref_dh_error.restype = ctypes.c_char_p
+        self.disc = disc
+        bcs = (ctypes.c_int * 5)(disc.frontBC, disc.rightBC, disc.backBC, disc.leftBC, disc.topBC)
+        h = ctypes.c_void_p()
+        d = ctypes.c_double
+        code = L.ref_dh_create(d(disc.omega), disc.nx, disc.ny, disc.nz, d(disc.wx), d(disc.wy), d(disc.wz), bcs,
+                               disc.bx, disc.by, disc.bz, d(disc.sigmax), d(disc.sigmay), d(disc.sigmaz), d(damping),
+                               planes_per_panel, cutoff, ctypes.byref(h))
+        if code:
+            raise RuntimeError(L.ref_dh_error().decode())
+        self._h = h
+        self.N = disc.nx * disc.ny * disc.nz
+        self.trees = self._recorded_trees()
+
+    def _recorded_trees(self):
+        """The elimination trees the constructor built for Clique's symbolic
+        analysis (bottom, leftover inner if any, top): per tree (info, lower)
+        with info rows (offset, size, parent, original lower-structure size)
+        and lower the list of each node's original lower structure."""
+        L = lib()
+        out = []
+        for t in range(3):
+            n, nl = ctypes.c_int(), ctypes.c_int()
+            if L.ref_dh_tree(t, ctypes.byref(n), ctypes.byref(nl), None, None):
+                break
+            info = np.zeros(4 * n.value, dtype=np.int32)
+            low = np.zeros(max(nl.value, 1), dtype=np.int32)
+            L.ref_dh_tree(t, ctypes.byref(n), ctypes.byref(nl), info.ctypes.data_as(ctypes.c_void_p),
+                          low.ctypes.data_as(ctypes.c_void_p))
+            info = info.reshape(n.value, 4)
+            ends = np.cumsum(info[:, 3])
+            out.append((info, [low[e - c:e] for e, c in zip(ends, info[:, 3])]))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ref_dh_destroy(self._h)
+            self._h = None
+
+    def _call(self, fn, *args):
+        if fn(self._h, *args):
+            raise RuntimeError(lib().ref_dh_error().decode())
+
+    def geometry(self):
+        """(num_panels, 3) int array: lowest v, depth, padding per panel."""
+        n = ctypes.c_int()
+        self._call(lib().ref_dh_geometry, ctypes.byref(n), None)
+        out = np.zeros(3 * n.value, dtype=np.int32)
+        self._call(lib().ref_dh_geometry, ctypes.byref(n), out.ctypes.data_as(ctypes.c_void_p))
+        return out.reshape(n.value, 3)
+
+    def local_to_natural(self):
+        out = np.zeros(self.N, dtype=np.int32)
+        self._call(lib().ref_dh_local_to_natural, out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def rows(self, velocity):
+        """(row offsets, complex entries) of the global rows in the
+        reference's order for a natural-order velocity."""
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        nnz = ctypes.c_int()
+        self._call(lib().ref_dh_rows, v.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nnz), None, None)
+        ro = np.zeros(self.N + 1, dtype=np.int32)
+        ent = np.zeros(nnz.value, dtype=np.complex128)
+        self._call(lib().ref_dh_rows, v.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nnz),
+                   ro.ctypes.data_as(ctypes.c_void_p), ent.ctypes.data_as(ctypes.c_void_p))
+        return ro, ent
+
+    def global_operator_natural(self, velocity):
+        """The global operator as a scipy CSR matrix in natural order: row
+        entries in FormGlobalRow's order (centre, then the -x, +x, -y, +y,
+        -v, +v neighbours that exist; v = nz - 1 - z)."""
+        import scipy.sparse as sp
+        ro, ent = self.rows(velocity)
+        nat = self.local_to_natural()
+        nx, ny, nz = self.disc.nx, self.disc.ny, self.disc.nz
+        x, y, z = nat % nx, (nat // nx) % ny, nat // (nx * ny)
+        v = nz - 1 - z
+        steps = [(x > 0, -1), (x + 1 < nx, 1), (y > 0, -nx), (y + 1 < ny, nx), (v > 0, nx * ny),
+                 (v + 1 < nz, -nx * ny)]
+        cols = np.zeros(ent.size, dtype=np.int64)
+        pos = ro[:-1].astype(np.int64).copy()
+        cols[pos] = nat
+        pos += 1
+        for have, step in steps:
+            cols[pos[have]] = nat[have] + step
+            pos[have] += 1
+        if not np.array_equal(pos, ro[1:]):
+            raise RuntimeError("row lengths do not match the stencil")
+        rows = np.repeat(nat, np.diff(ro))
+        return sp.csr_matrix((ent, (rows, cols)), shape=(self.N, self.N))
+
+    def stretch(self, which, idx, v_offset=0):
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        out = np.zeros(idx.size, dtype=np.complex128)
+        self._call(lib().ref_dh_stretch, which, idx.size, idx.ctypes.data_as(ctypes.c_void_p), v_offset,
+                   out.ctypes.data_as(ctypes.c_void_p))
+        return out

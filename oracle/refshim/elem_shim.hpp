@@ -61,8 +61,8 @@ template <typename T>
 inline T Abs(T x) { return std::abs(x); }
 
 template <typename T>
-inline void SwapClear(std::vector<T>& v) {
-    std::vector<T>().swap(v);
+inline void SwapClear(T& x) {
+    T().swap(x);
 }
 
 inline void EnsureDirExists(const char* path, mode_t mode = 0777) {
