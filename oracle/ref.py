@@ -198,3 +198,23 @@ class RefHelmholtz:
         self._call(lib().ref_dh_stretch, which, idx.size, idx.ctypes.data_as(ctypes.c_void_p), v_offset,
                    out.ctypes.data_as(ctypes.c_void_p))
         return out
+
+    def solve(self, velocity, orc, B, m=20, rel_tol=1e-4):
+        """The reference's own Solve (solve.hpp:12-611) of the right-hand
+        sides B (natural order, (nz, ny, nx, k) complex128) on a copy, with
+        the global rows formed from `velocity` and the panel solves of the
+        initialized oracle `orc` in place of Clique's.  Returns (X, log,
+        iterations): what the reference printed, and its GMRES step count
+        (its "finished iteration" lines plus the converged one)."""
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        X = np.ascontiguousarray(B, dtype=np.complex128).copy()
+        k = X.size // self.N
+        L = lib()
+        L.ref_dh_log.restype = ctypes.c_char_p
+        code = L.ref_dh_solve(self._h, orc._h, v.ctypes.data_as(ctypes.c_void_p), X.ctypes.data_as(ctypes.c_void_p),
+                              k, m, ctypes.c_double(rel_tol))
+        log = L.ref_dh_log().decode()
+        if code:
+            raise RuntimeError(L.ref_dh_error().decode())
+        its = log.count("finished iteration") + log.count("converged with relative tolerance")
+        return X, log, its

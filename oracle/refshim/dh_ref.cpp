@@ -2,7 +2,8 @@
 //
 // C entry points around the reference's own psp::DistHelmholtz on one
 // process (include/psp/dist_helmholtz.hpp and dist_helmholtz/*.hpp,
-// compiled unchanged from the reference tree against clique_shim.hpp):
+// compiled unchanged from the reference tree with its psp.hpp, against the
+// stand-in for Clique and Elemental in clique.hpp):
 //   the constructor (main.hpp:12-441): panel geometry (PanelV, PanelDepth,
 //     PanelPadding, main.hpp:728-790) and the global nested-dissection
 //     ordering (localToNaturalMap_, main.hpp:1423-1477);
@@ -14,20 +15,74 @@
 // reproduced (a no-op here), so nothing that needs the frontal structure is
 // exposed.  The members are private in the reference; this translation unit
 // opens them to call them as a test harness.
-#include "clique_shim.hpp"
-#include "psp/discretization.hpp"
-#include "psp/dist_uniform_grid.hpp"
+#include "clique.hpp"
 #define private public
-#include "psp/dist_helmholtz.hpp"
+#include "psp.hpp"
 #undef private
 
 #include <complex>
 #include <memory>
 #include <string>
 
+// The oracle's panel solve (oracle/psp_oracle.cpp): B := T_p B on panel p's
+// planes of a natural-order grid of k interleaved right-hand sides.
+extern "C" int oracle_solve_panel(void* h, double* grid, int k, int p);
+
 namespace {
-std::string g_error;
+std::string g_error, g_log;
 typedef psp::DistHelmholtz<double> DH;
+typedef std::complex<double> Cd;
+
+// The global rows exactly as Initialize forms them (initialize_finalize.hpp:
+// 340-375) for a natural-order velocity.
+void FormRows(DH& H, const double* velocity) {
+    const int nx = H.disc_.nx, ny = H.disc_.ny, nz = H.disc_.nz;
+    psp::DistUniformGrid<double> vel(nx, ny, nz, 0, 1);
+    std::copy(velocity, velocity + (size_t)nx * ny * nz, vel.Buffer());
+    std::vector<double> myGlobalVelocity;
+    std::vector<int> offsets;
+    H.GetGlobalVelocity(vel, myGlobalVelocity, offsets);
+    H.localEntries_.resize(H.localRowOffsets_.back());
+    for (int iLocal = 0; iLocal < H.localSize_; ++iLocal) {
+        const int naturalIndex = H.localToNaturalMap_[iLocal];
+        const int x = naturalIndex % nx, y = (naturalIndex / nx) % ny, z = naturalIndex / (nx * ny);
+        const int proc = vel.OwningProcess(x, y, z);
+        const double alpha = myGlobalVelocity[offsets[proc]++];
+        H.FormGlobalRow(alpha, x, y, (nz - 1) - z, H.localRowOffsets_[iLocal]);
+    }
+}
+
+// T_i applied to the right-hand sides of panel i, laid out as the
+// reference's SolvePanel hands them to Clique (solve.hpp:736-822): node by
+// node of the panel's elimination order, each node's padding rows first
+// (zero), then its physical rows, which are the reference's rows
+// LocalPanelOffset(i) onwards.  The physical rows go through a natural-order
+// grid to the oracle's panel solve and come back the same way.
+void OraclePanelSolve(const DH& H, void* oracle, int i, cliq::DistNodalMultiVec<Cd>& X) {
+    const cliq::DistSymmInfo& info = H.PanelAnalysis(i);
+    const int padding = H.PanelPadding(i), depth = H.PanelDepth(i);
+    const int k = X.localNodes.empty() ? 0 : X.localNodes[0].Width();
+    const size_t N = (size_t)H.disc_.nx * H.disc_.ny * H.disc_.nz;
+    std::vector<Cd> grid(N * k, Cd(0));
+    for (int pass = 0; pass < 2; ++pass) {
+        int bOff = H.LocalPanelOffset(i);
+        for (size_t t = 0; t < info.localNodes.size(); ++t) {
+            const int size = info.localNodes[t].size;
+            const int paddingSize = (size / (padding + depth)) * padding;
+            elem::Matrix<Cd>& mat = X.localNodes[t];
+            for (int r = 0; r < size - paddingSize; ++r) {
+                Cd* g = &grid[(size_t)H.localToNaturalMap_[bOff + r] * k];
+                for (int c = 0; c < k; ++c) {
+                    if (pass == 0) g[c] = mat.Get(paddingSize + r, c);
+                    else mat.Set(paddingSize + r, c, g[c]);
+                }
+            }
+            bOff += size - paddingSize;
+        }
+        if (pass == 0 && oracle_solve_panel(oracle, reinterpret_cast<double*>(grid.data()), k, i))
+            throw std::runtime_error("oracle panel solve failed");
+    }
+}
 
 template <typename F>
 int Guard(F&& f) {
@@ -56,7 +111,7 @@ int ref_dh_create(double omega, int nx, int ny, int nz, double wx, double wy, do
         disc.sigmax = sigmax;
         disc.sigmay = sigmay;
         disc.sigmaz = sigmaz;
-        psp::cliq::RecordedTrees().clear();
+        cliq::RecordedTrees().clear();
         *out = new DH(disc, 0, damping, planes, cutoff);
     });
 }
@@ -68,7 +123,7 @@ int ref_dh_create(double omega, int nx, int ny, int nz, double wx, double wy, do
 // null (counts only).
 int ref_dh_tree(int t, int* numNodes, int* numLower, int* info, int* lower) {
     return Guard([&] {
-        const auto& trees = psp::cliq::RecordedTrees();
+        const auto& trees = cliq::RecordedTrees();
         if (t < 0 || t >= (int)trees.size()) throw std::logic_error("no such elimination tree");
         const auto& T = trees[t];
         *numNodes = (int)T.size();
@@ -87,7 +142,12 @@ int ref_dh_tree(int t, int* numNodes, int* numLower, int* info, int* lower) {
     });
 }
 
-void ref_dh_destroy(void* h) { delete static_cast<DH*>(h); }
+void ref_dh_destroy(void* h) {
+    DH* H = static_cast<DH*>(h);
+    for (auto* f : H->fullInnerFacts_) delete f;
+    H->fullInnerFacts_.clear();
+    delete H;
+}
 
 // Per panel: lowest v, depth, padding (v = nz - 1 - z).
 int ref_dh_geometry(void* h, int* numPanels, int* info) {
@@ -111,6 +171,51 @@ int ref_dh_local_to_natural(void* h, int* out) {
     });
 }
 
+// The reference's own Solve (solve.hpp:12-611: pull, GMRES(m) with its
+// sweep Precondition, Multiply and Givens updates, push) of the k
+// right-hand sides in `grid` (natural order, interleaved), in place, with
+// the global rows formed from `velocity` and Clique's panel solves replaced
+// by those of `oracle` (an initialized oracle handle of the same problem).
+// What the reference prints goes to ref_dh_log().
+int ref_dh_solve(void* h, void* oracle, const double* velocity, double* grid, int k, int m, double relTol) {
+    return Guard([&] {
+        DH& H = *static_cast<DH*>(h);
+        FormRows(H, velocity);
+        // Initialize allocates one front tree per full inner panel; the
+        // panel solver tells panels apart by these objects.
+        std::map<const void*, int> panelOf;
+        if ((int)H.fullInnerFacts_.size() != H.numFullInnerPanels_) {
+            H.fullInnerFacts_.clear();
+            for (int j = 0; j < H.numFullInnerPanels_; ++j)
+                H.fullInnerFacts_.push_back(new cliq::DistSymmFrontTree<Cd>);
+        }
+        for (int i = H.numPanels_ - 1; i >= 0; --i) panelOf[&H.PanelFactorization(i)] = i;
+        cliq::InstalledPanelSolver() = [&](const void* fact, cliq::DistNodalMultiVec<Cd>& X) {
+            OraclePanelSolve(H, oracle, panelOf.at(fact), X);
+        };
+        const int nx = H.disc_.nx, ny = H.disc_.ny, nz = H.disc_.nz;
+        psp::DistUniformGrid<Cd> B(nx, ny, nz, 0, k);
+        const size_t n = (size_t)nx * ny * nz * k;
+        std::copy(reinterpret_cast<const Cd*>(grid), reinterpret_cast<const Cd*>(grid) + n, B.Buffer());
+        std::ostringstream log;
+        std::streambuf* old = std::cout.rdbuf(log.rdbuf());
+        try {
+            H.Solve(B, m, relTol);
+        } catch (...) {
+            std::cout.rdbuf(old);
+            g_log = log.str();
+            cliq::InstalledPanelSolver() = nullptr;
+            throw;
+        }
+        std::cout.rdbuf(old);
+        g_log = log.str();
+        cliq::InstalledPanelSolver() = nullptr;
+        std::copy(B.LockedBuffer(), B.LockedBuffer() + n, reinterpret_cast<Cd*>(grid));
+    });
+}
+
+const char* ref_dh_log() { return g_log.c_str(); }
+
 // Global rows for a natural-order velocity: rowOffsets (N + 1 entries) and
 // the complex entries of every row (center, then the -x, +x, -y, +y, -v, +v
 // neighbours that exist), as Initialize forms them.  With entries null only
@@ -118,22 +223,9 @@ int ref_dh_local_to_natural(void* h, int* out) {
 int ref_dh_rows(void* h, const double* velocity, int* nnz, int* rowOffsets, double* entries) {
     return Guard([&] {
         DH& H = *static_cast<DH*>(h);
-        const int nx = H.disc_.nx, ny = H.disc_.ny, nz = H.disc_.nz;
         *nnz = H.localRowOffsets_.back();
         if (!entries) return;
-        psp::DistUniformGrid<double> vel(nx, ny, nz, 0, 1);
-        std::copy(velocity, velocity + (size_t)nx * ny * nz, vel.Buffer());
-        std::vector<double> myGlobalVelocity;
-        std::vector<int> offsets;
-        H.GetGlobalVelocity(vel, myGlobalVelocity, offsets);
-        H.localEntries_.resize(H.localRowOffsets_.back());
-        for (int iLocal = 0; iLocal < H.localSize_; ++iLocal) {
-            const int naturalIndex = H.localToNaturalMap_[iLocal];
-            const int x = naturalIndex % nx, y = (naturalIndex / nx) % ny, z = naturalIndex / (nx * ny);
-            const int proc = vel.OwningProcess(x, y, z);
-            const double alpha = myGlobalVelocity[offsets[proc]++];
-            H.FormGlobalRow(alpha, x, y, (nz - 1) - z, H.localRowOffsets_[iLocal]);
-        }
+        FormRows(H, velocity);
         std::copy(H.localRowOffsets_.begin(), H.localRowOffsets_.end(), rowOffsets);
         std::copy(H.localEntries_.begin(), H.localEntries_.end(), reinterpret_cast<std::complex<double>*>(entries));
     });

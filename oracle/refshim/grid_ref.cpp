@@ -2,7 +2,8 @@
 //
 // C entry points around the reference's own psp::DistUniformGrid
 // (include/psp/dist_uniform_grid.hpp, compiled unchanged from the reference
-// tree against the one-process shim in elem_shim.hpp), so tests can check
+// tree with its psp.hpp, against the one-process stand-in for Clique and
+// Elemental in clique.hpp), so tests can check
 // the numpy restatement in oracle/grid_io.py and the product's grid kernels
 // against the reference code itself:
 //   SequentialLoad  dist_uniform_grid.hpp:349-482
@@ -13,8 +14,8 @@
 // (x fastest), numScalars entries interleaved per point; complex entries as
 // (re, im) double pairs.  Every function returns 0, or 1 with the
 // exception's text in ref_grid_error().
-#include "elem_shim.hpp"
-#include "psp/dist_uniform_grid.hpp"
+#include "clique.hpp"
+#include "psp.hpp"
 
 #include <algorithm>
 #include <complex>

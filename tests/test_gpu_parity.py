@@ -139,6 +139,11 @@ def test_reference_error_conventions(product_lib):
         H.precondition(w.rhs)
 
 
+def _ref_available():
+    from oracle import ref
+    return ref.available()
+
+
 @pytest.fixture(scope="module")
 def bump_fp64(product_lib):
     """The full FP64 reference case (50^3 grid with a 5-point PML, 4
@@ -169,6 +174,23 @@ def test_unit_cube_bump_matches_oracle(bump_fp64):
         rr = max(np.linalg.norm(R[..., r]) / np.linalg.norm(w.rhs[..., r]) for r in range(w.k))
         assert rr < 1e-4
     assert abs(st["final_max_rel_resid"] - sto["final_max_rel_resid"]) < 1e-10
+
+
+@pytest.mark.skipif(not _ref_available(), reason="the reference's DistHelmholtz was not built")
+def test_unit_cube_bump_matches_reference_solve(bump_fp64):
+    """The plain FP64 path against the reference's own Solve of the 50^3
+    case (solve.hpp:12-611 compiled unchanged on one process, its GMRES,
+    sweep and global rows; oracle/_ref): the same GMRES step count and a
+    relative wavefield difference of at most 1e-6 at equal tolerance.  Only
+    Clique's panel factorization and solve, absent from the reference tree,
+    come from the oracle there."""
+    from oracle import ref
+    w, O, Xo, sto, X, st = bump_fp64
+    Xr, log, its = ref.RefHelmholtz(w.disc).solve(w.velocity, O, w.rhs, 20, 1e-4)
+    assert "converged with relative tolerance" in log
+    assert st["iterations"] == its
+    assert rel(X, Xr) < 1e-6
+    assert rel(Xo, Xr) < 1e-12
 
 
 def test_unit_cube_bump_matches_direct_solve(bump_fp64):
