@@ -70,6 +70,8 @@ def parse():
                     help="time grid ingest: a ZYX-ordered velocity file loaded to the device and resampled 2x")
     ap.add_argument("--sweep-probe", action="store_true",
                     help="profiling driver: Initialize (mixed) + two sweeps on the device, then exit")
+    ap.add_argument("--stencil-probe", action="store_true",
+                    help="profiling driver: Initialize (mixed) + three global operator applications, then exit")
     return ap.parse_args()
 
 
@@ -116,6 +118,19 @@ def sweep_probe(args):
         H.precondition_device(B)
     torch.cuda.synchronize()
     print("sweep probe done", args.config, flush=True)
+
+
+def stencil_probe(args):
+    import torch
+    import psp_b200 as P
+    w = workload(args.config)
+    H = P.DistHelmholtz(w.disc)
+    H.Initialize(torch.from_numpy(w.velocity.reshape(-1)).cuda(), precision=P.MIXED)
+    B = w.rhs_torch("cuda")
+    for _ in range(3):
+        H.multiply_device(B)
+    torch.cuda.synchronize()
+    print("stencil probe done", args.config, flush=True)
 
 
 def load_peaks():
@@ -622,6 +637,8 @@ def main():
         return grid_probe(args)
     if args.sweep_probe:
         return sweep_probe(args)
+    if args.stencil_probe:
+        return stencil_probe(args)
     if args.impl == "reference":
         return main_reference(args)
     import torch
