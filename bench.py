@@ -480,9 +480,10 @@ def profile_block(H, w, kb, stream):
 
 
 # DRAM bytes per algorithmic byte of a sweep launch, from one ncu capture
-# of the forward tensor-core sweep kernel on a profiling-sized member of the
-# workload family (profiles/)
-SWEEP_TRAFFIC_RATIO = (20.43e6 + 2.8e3) / 16.84e6
+# of each 32-column tensor-core sweep kernel on the differentiation workload
+# (forward depth 8 and backward depth 2: 96.7 + 29.0 MB of DRAM traffic for
+# 73.4 + 30.5 MB of algorithmic bytes; profiles/)
+SWEEP_TRAFFIC_RATIO = (96.7e6 + 29.0e6) / (73.4e6 + 30.5e6)
 
 
 def roofline_entry(name, p, peaks):
@@ -510,8 +511,8 @@ def roofline_from_profile(prof, peaks):
     out = roofline_entry(name, kernels[name], peaks)
     if name == "solve_gemm":
         out["traffic"] = SWEEP_TRAFFIC_RATIO * kernels[name]["bytes"] / max(kernels[name]["launches"], 1)
-        out["traffic_note"] = ("dram__bytes_read+write per launch, scaled from an ncu capture of the forward "
-                               "sweep kernel (1.21x algorithmic)")
+        out["traffic_note"] = ("dram__bytes_read+write per launch, scaled from ncu captures of the 32-column "
+                               "forward and backward sweep kernels (1.21x algorithmic)")
     else:
         out["traffic"] = None
     others = {n: roofline_entry(n, kernels[n], peaks) for n in ("stencil", "gmres_vector") if n in kernels}
