@@ -104,17 +104,9 @@ __device__ __forceinline__ bool Wait(uint64_t* mbar, uint32_t parity, Sync& S, i
 // an accumulator.
 __device__ __forceinline__ int StagesOf(const GemmTcTile& t) { return t.nk > 0 ? (t.nk + kSK - 1) / kSK : 1; }
 
-// Head rounded to tf32 (11 significant bits, ties away from zero) by integer
-// arithmetic on the bit pattern; the tail x - hi is exact in fp32 and the
-// MMA reads its top 11 bits, so x ~= hi + lo to ~2^-21 relative.
-__device__ __forceinline__ void SplitFast(float x, float& hi, float& lo) {
-    hi = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-    lo = x - hi;
-}
-
 __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
-    SplitFast(x.re, hi.x, lo.x);
-    SplitFast(x.im, hi.y, lo.y);
+    umma::SplitTf32Fast(x.re, hi.x, lo.x);
+    umma::SplitTf32Fast(x.im, hi.y, lo.y);
 }
 
 // ------------------------------------------------------------------ converters

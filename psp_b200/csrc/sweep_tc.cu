@@ -336,8 +336,8 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
 
 // Splits x into tf32 head and tail.
 __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
-    umma::SplitTf32(x.re, hi.x, lo.x);
-    umma::SplitTf32(x.im, hi.y, lo.y);
+    umma::SplitTf32Fast(x.re, hi.x, lo.x);
+    umma::SplitTf32Fast(x.im, hi.y, lo.y);
 }
 
 // Issues this converter thread's own copies of the cursor's stage (its two

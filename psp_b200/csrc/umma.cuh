@@ -323,6 +323,15 @@ __device__ __forceinline__ void TmemLoad16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Split x into a tf32 head rounded by integer arithmetic on the bit pattern
+// (11 significant bits, ties away from zero) and the exact fp32 tail x - hi,
+// of which the MMA reads the top 11 bits: x ~= hi + lo to ~2^-21 relative,
+// in three integer/FP32 operations (no conversion instructions).
+__device__ __forceinline__ void SplitTf32Fast(float x, float& hi, float& lo) {
+    hi = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+    lo = x - hi;
+}
+
 // Split x into a tf32 head and a tf32 tail: x ~= hi + lo to ~2^-22 relative.
 __device__ __forceinline__ void SplitTf32(float x, float& hi, float& lo) {
     uint32_t h;
