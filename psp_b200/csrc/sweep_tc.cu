@@ -433,10 +433,15 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
         Split2(b, h, l);
         const uint32_t o0 = umma::Sw128Offset(2 * nn, kc >> 1) + (kc & 1) * 8;
         const uint32_t o1 = umma::Sw128Offset(2 * nn + 1, kc >> 1) + (kc & 1) * 8;
-        *reinterpret_cast<float2*>(bHi + o0) = make_float2(h.x, -h.y);
-        *reinterpret_cast<float2*>(bHi + o1) = make_float2(h.y, h.x);
-        *reinterpret_cast<float2*>(bLo + o0) = make_float2(l.x, -l.y);
-        *reinterpret_cast<float2*>(bLo + o1) = make_float2(l.y, l.x);
+        // lanes with bit 2 of n set store their odd row first, so each store
+        // instruction covers all eight swizzle phases of a row group
+        const bool odd = (nn >> 2) & 1;
+        const float2 hr = make_float2(h.x, -h.y), hi = make_float2(h.y, h.x);
+        const float2 lr = make_float2(l.x, -l.y), li = make_float2(l.y, l.x);
+        *reinterpret_cast<float2*>(bHi + (odd ? o1 : o0)) = odd ? hi : hr;
+        *reinterpret_cast<float2*>(bHi + (odd ? o0 : o1)) = odd ? hr : hi;
+        *reinterpret_cast<float2*>(bLo + (odd ? o1 : o0)) = odd ? li : lr;
+        *reinterpret_cast<float2*>(bLo + (odd ? o0 : o1)) = odd ? lr : li;
     }
 }
 
