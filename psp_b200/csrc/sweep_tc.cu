@@ -340,6 +340,20 @@ __device__ __forceinline__ void Split2(c32 x, float2& hi, float2& lo) {
     umma::SplitTf32Fast(x.im, hi.y, lo.y);
 }
 
+// The right-hand-side entry (kc, nn) of a stage that converter thread ct
+// copies and converts in its j-th slot: consecutive threads take
+// consecutive columns, and columns 8-15 of every 16 take the neighbouring
+// K row, so that a warp's B' stores use both 8-byte halves of a 16-byte
+// chunk as well as all eight swizzle phases (two wavefronts per store, the
+// least for 256 bytes); its copies still read whole 32-byte sectors.  The
+// entry sits at kc NC + nn in the group's copy slot.
+template <int NC>
+__device__ __forceinline__ void OwnEntry(int ct, int j, int& kc, int& nn) {
+    const int e = ct + j * kGroupThreads;
+    nn = e % NC;
+    kc = (e / NC) ^ ((nn >> 3) & 1);
+}
+
 // Issues this converter thread's own copies of the cursor's stage (its two
 // B entries; backward also its eight 16-byte A chunks, zero-filled outside
 // the tile), commits one copy group and moves the cursor to the group's
@@ -361,8 +375,9 @@ __device__ __forceinline__ void IssueOwn(LoadCursor<kFwd>& cur, unsigned char* o
     const int kBase = cur.KBase();
 #pragma unroll
     for (int j = 0; j < kStageK * NC / kGroupThreads; ++j) {
-        const int e = ct + j * kGroupThreads;
-        const int kc = e / NC, nn = e % NC;
+        int kc, nn;
+        OwnEntry<NC>(ct, j, kc, nn);
+        const int e = kc * NC + nn;
         const int kk = kBase + kc;
         const bool ok = kk < m.ke && nn < ncol;
         if (kFwd) {
@@ -426,8 +441,9 @@ __device__ __forceinline__ void ConvertStage(unsigned char* P, const unsigned ch
     unsigned char* bLo = bHi + C::kBPlane;
 #pragma unroll
     for (int j = 0; j < kStageK * NC / kGroupThreads; ++j) {
-        const int e = ct + j * kGroupThreads;
-        const int kc = e / NC, nn = e % NC;
+        int kc, nn;
+        OwnEntry<NC>(ct, j, kc, nn);
+        const int e = kc * NC + nn;
         const c32 b = kFwd ? rb[e] + rb[kStageK * NC + e] + rb[2 * kStageK * NC + e] : rb[e];
         float2 h, l;
         Split2(b, h, l);
