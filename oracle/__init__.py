@@ -125,6 +125,21 @@ class Oracle:
         lib().oracle_stretch(self._h, which, idx.size, _ptr(idx, ctypes.c_int), v_offset, _ptr(out.view(np.float64)))
         return out
 
+    def panel_front(self, velocity, p, t):
+        """Node t of panel p: the first s columns of its front, (s+u) x s
+        complex128, as assembled from the velocity before any update."""
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        L = lib()
+        L.oracle_panel_front.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_double)]
+        s, u = ctypes.c_int(), ctypes.c_int()
+        if L.oracle_panel_front(self._h, _ptr(v), p, t, ctypes.byref(s), ctypes.byref(u), None):
+            raise ValueError("no such panel or node")
+        out = np.zeros(((s.value + u.value) * s.value), dtype=np.complex128)
+        L.oracle_panel_front(self._h, _ptr(v), p, t, ctypes.byref(s), ctypes.byref(u), _ptr(out.view(np.float64)))
+        return out.reshape(s.value, s.value + u.value).T
+
     def nd_to_natural(self):
         out = np.zeros(self.N, dtype=np.int32)
         lib().oracle_nd_to_natural(self._h, _ptr(out, ctypes.c_int))

@@ -491,21 +491,20 @@ void PartialLDL(C* F, int n, int s) {
 }
 
 // FillPanelFronts (initialize_finalize.hpp:1284-1394) with
-// FormLowerColumnOfNode (589-806), then the multifrontal factorization that
-// cliq::LDL performs (initialize_finalize.hpp:145-150).
-void FactorPanel(Solver& S, int p, const double* vel) {
+// The first s columns of node t's front of panel p as FillPanelFronts
+// forms them (initialize_finalize.hpp:1284-1340 with FormLowerColumnOfNode,
+// 589-806): the padded panel's operator with the damped frequency and the
+// artificial PML, on and below the diagonal; column j at F + j ld.
+void AssembleFront(const Solver& S, int p, size_t t, const double* vel, C* F, int ld) {
     const int nx = S.disc.nx, ny = S.disc.ny;
     const PanelTree& T = S.trees[PanelClass(S, p)];
     const int vSize = T.vSize;
     const int vOffset = PanelV(S, p) - PanelPadding(S, p);
     const C shiftedOmega(S.disc.omega, S.damping);
-    std::vector<Front>& fr = S.fronts[p];
-    fr.assign(T.nodes.size(), Front());
-    std::vector<std::vector<C>> updates(T.nodes.size());
-    for (size_t t = 0; t < T.nodes.size(); ++t) {
-        const Node& node = T.nodes[t];
-        const int s = node.size, u = (int)node.lower.size(), n = s + u;
-        std::vector<C> F((size_t)n * n, C(0));
+    const Node& node = T.nodes[t];
+    const int s = node.size;
+    {
+        const int n = ld;
         for (int j = 0; j < s; ++j) {
             const int pn = T.ndToNat[node.off + j];
             const int x = pn % nx, y = (pn / nx) % ny, vLocal = pn / (nx * ny);
@@ -514,7 +513,7 @@ void FactorPanel(Solver& S, int p, const double* vel) {
             const Stencil st = StencilTerms(S, alpha, x, y, s3InvArtificial(S, v - 1, vOffset),
                                             s3InvArtificial(S, v, vOffset), s3InvArtificial(S, v + 1, vOffset),
                                             shiftedOmega);
-            C* col = F.data() + (size_t)j * n;
+            C* col = F + (size_t)j * n;
             col[j] = st.center;
             auto put = [&](int xx, int yy, int vl, C val) {
                 const int nested = RI(S, xx, yy, vl, vSize);
@@ -534,6 +533,21 @@ void FactorPanel(Solver& S, int p, const double* vel) {
             if (vLocal > 0) put(x, y, vLocal - 1, -st.vL);
             if (vLocal + 1 < vSize) put(x, y, vLocal + 1, -st.vR);
         }
+    }
+}
+
+// FillPanelFronts (above), then the multifrontal factorization that
+// cliq::LDL performs (initialize_finalize.hpp:145-150).
+void FactorPanel(Solver& S, int p, const double* vel) {
+    const PanelTree& T = S.trees[PanelClass(S, p)];
+    std::vector<Front>& fr = S.fronts[p];
+    fr.assign(T.nodes.size(), Front());
+    std::vector<std::vector<C>> updates(T.nodes.size());
+    for (size_t t = 0; t < T.nodes.size(); ++t) {
+        const Node& node = T.nodes[t];
+        const int s = node.size, u = (int)node.lower.size(), n = s + u;
+        std::vector<C> F((size_t)n * n, C(0));
+        AssembleFront(S, p, t, vel, F.data(), n);
         // extend-add of the children's Schur complements
         for (int c = 0; c < node.numChildren; ++c) {
             const int ch = node.children[c];
@@ -820,6 +834,26 @@ int oracle_stretch(void* h, int which, int n, const int* idx, int vOffset, doubl
                                : s3InvArtificial(S, idx[i], vOffset);
         out[2 * i] = c.real();
         out[2 * i + 1] = c.imag();
+    }
+    return 0;
+}
+
+// Node t of panel p: its pivot count *s and structure size *u, and (out
+// non-null) the first s columns of its front, (s + u) x s column-major as
+// (re, im) pairs, as assembled from `velocity` before any update is added.
+int oracle_panel_front(void* h, const double* velocity, int p, int t, int* s, int* u, double* out) {
+    const Solver& S = *(const Solver*)h;
+    if (p < 0 || p >= S.numPanels) return 1;
+    const PanelTree& T = S.trees[PanelClass(S, p)];
+    if (t < 0 || t >= (int)T.nodes.size()) return 1;
+    const Node& node = T.nodes[t];
+    *s = node.size;
+    *u = (int)node.lower.size();
+    if (out) {
+        const int n = *s + *u;
+        std::vector<C> F((size_t)n * n, C(0));
+        AssembleFront(S, p, (size_t)t, velocity, F.data(), n);
+        std::memcpy(out, F.data(), sizeof(C) * (size_t)n * *s);
     }
     return 0;
 }

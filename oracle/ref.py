@@ -218,3 +218,16 @@ class RefHelmholtz:
             raise RuntimeError(L.ref_dh_error().decode())
         its = log.count("finished iteration") + log.count("converged with relative tolerance")
         return X, log, its
+
+    def panel_front(self, velocity, p, t):
+        """Node t of panel p's front as the reference's Initialize fills it
+        (GetPanelVelocity, FillPanelFronts): the first s columns, (s+u) x s
+        complex128, before any update is added."""
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        s, u = ctypes.c_int(), ctypes.c_int()
+        self._call(lib().ref_dh_panel_front, v.ctypes.data_as(ctypes.c_void_p), p, t, ctypes.byref(s),
+                   ctypes.byref(u), None)
+        out = np.zeros((s.value + u.value) * s.value, dtype=np.complex128)
+        self._call(lib().ref_dh_panel_front, v.ctypes.data_as(ctypes.c_void_p), p, t, ctypes.byref(s),
+                   ctypes.byref(u), out.ctypes.data_as(ctypes.c_void_p))
+        return out.reshape(s.value, s.value + u.value).T

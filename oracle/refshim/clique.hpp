@@ -15,9 +15,10 @@
 //   conjugated Dot, and ComputeGivens with LAPACK zlartg's convention
 //   (c real, [c s; -conj(s) c] [f; g] = [r; 0]).
 // * Clique: its tree and front types as plain structs.  Its symbolic
-//   analysis records the elimination trees the reference hands it and sets
-//   each node's offset and size, which is all the reference's panel solve
-//   reads.  Clique's multifrontal factorization and solve are not in the
+//   analysis records the elimination trees the reference hands it and
+//   computes the node structures from them (restating Clique's published
+//   symbolic factorization), which the reference's panel assembly and panel
+//   solve read.  Clique's multifrontal factorization and solve are not in the
 //   reference tree: LDL throws, and Solve calls a panel solver that the
 //   harness installs (the oracle's, oracle/psp_oracle.cpp), so the
 //   reference's sweep and GMRES run around it.
@@ -198,6 +199,7 @@ public:
     void Align(int, int) {}
     int LocalHeight() const { return this->Height(); }
     int LocalWidth() const { return this->Width(); }
+    void SetLocal(int i, int j, T x) { this->Set(i, j, x); }
 };
 
 template <typename T>
@@ -379,7 +381,7 @@ struct SymmFront {
 };
 template <typename F>
 struct DistSymmFront {
-    elem::DistMatrix<F> front;
+    elem::DistMatrix<F> front, front2dL;
 };
 template <typename F>
 struct DistSymmFrontTree {
@@ -404,15 +406,36 @@ inline std::vector<std::vector<SymmNode>>& RecordedTrees() {
     static std::vector<std::vector<SymmNode>> trees;
     return trees;
 }
-// Clique's symbolic analysis computes each node's offset and size (and the
-// fill, which nothing here reads); the offsets and sizes are the tree's.
+// Clique's symbolic analysis (its published definition, restated): per
+// node, in postorder, the original lower structure sorted; the structure
+// after fill, the union of the original one and of the children's
+// structures less this node's own indices, sorted; and the position of each
+// original entry among the front's rows (own indices first, then the
+// structure).  The reference's panel assembly (FillPanelFronts) reads these.
 inline void SymmetricAnalysis(const DistSymmElimTree& eTree, DistSymmInfo& info, bool) {
+    const size_t n = eTree.localNodes.size();
     std::vector<SymmNode> t;
-    info.localNodes.assign(eTree.localNodes.size(), SymmNodeInfo());
-    for (size_t i = 0; i < eTree.localNodes.size(); ++i) {
-        t.push_back(*eTree.localNodes[i]);
-        info.localNodes[i].size = eTree.localNodes[i]->size;
-        info.localNodes[i].off = eTree.localNodes[i]->off;
+    info.localNodes.assign(n, SymmNodeInfo());
+    for (size_t i = 0; i < n; ++i) {
+        const SymmNode& node = *eTree.localNodes[i];
+        t.push_back(node);
+        SymmNodeInfo& ni = info.localNodes[i];
+        ni.size = node.size;
+        ni.off = node.off;
+        ni.origLowerStruct = node.lowerStruct;
+        std::sort(ni.origLowerStruct.begin(), ni.origLowerStruct.end());
+        ni.origLowerStruct.erase(std::unique(ni.origLowerStruct.begin(), ni.origLowerStruct.end()),
+                                 ni.origLowerStruct.end());
+        std::set<int> fill(ni.origLowerStruct.begin(), ni.origLowerStruct.end());
+        for (int c : node.children)
+            for (int x : info.localNodes[c].lowerStruct)
+                if (x < node.off || x >= node.off + node.size) fill.insert(x);
+        ni.lowerStruct.assign(fill.begin(), fill.end());
+        ni.origLowerRelInds.resize(ni.origLowerStruct.size());
+        for (size_t a = 0; a < ni.origLowerStruct.size(); ++a)
+            ni.origLowerRelInds[a] = node.size + int(std::lower_bound(ni.lowerStruct.begin(), ni.lowerStruct.end(),
+                                                                      ni.origLowerStruct[a]) -
+                                                     ni.lowerStruct.begin());
     }
     info.distNodes.assign(std::max<size_t>(1, eTree.distNodes.size()), DistSymmNodeInfo());
     RecordedTrees().push_back(t);
@@ -434,10 +457,9 @@ template <typename... A>
 inline void LDL(A&&...) {
     elem::LogicError("Clique's LDL is not part of this checker");
 }
+// On one rank no front is distributed: nothing to set up.
 template <typename... A>
-inline void InitializeDistLeaf(A&&...) {
-    elem::LogicError("Clique's InitializeDistLeaf is not part of this checker");
-}
+inline void InitializeDistLeaf(A&&...) {}
 // One rank: the received vector is the sent one.
 template <typename T>
 inline void SparseAllToAll(const std::vector<T>& sendBuf, const std::vector<int>& sendCounts,

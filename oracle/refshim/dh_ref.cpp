@@ -10,7 +10,10 @@
 //   the global sparse rows exactly as Initialize forms them
 //     (initialize_finalize.hpp:340-375): GetGlobalVelocity, then
 //     FormGlobalRow (527-587) for every row in the reference's order;
-//   the PML stretches s1Inv, s2Inv, s3Inv and s3InvArtificial (415-525).
+//   the PML stretches s1Inv, s2Inv, s3Inv and s3InvArtificial (415-525);
+//   the panel fronts as Initialize fills them (FillPanelFronts with
+//   FormLowerColumnOfNode, 589-806, 1284-1394), on node structures from
+//   the stand-in's symbolic analysis;
 // Clique's symbolic analysis, which the constructor also calls, is not
 // reproduced (a no-op here), so nothing that needs the frontal structure is
 // exposed.  The members are private in the reference; this translation unit
@@ -228,6 +231,38 @@ int ref_dh_rows(void* h, const double* velocity, int* nnz, int* rowOffsets, doub
         FormRows(H, velocity);
         std::copy(H.localRowOffsets_.begin(), H.localRowOffsets_.end(), rowOffsets);
         std::copy(H.localEntries_.begin(), H.localEntries_.end(), reinterpret_cast<std::complex<double>*>(entries));
+    });
+}
+
+// Node t of panel p's front as the reference's Initialize fills it
+// (GetPanelVelocity then FillPanelFronts, initialize_finalize.hpp:123-136,
+// 884-1044, 1284-1394): pivot count *s, structure size *u and, with out
+// non-null, the (s + u) x s column-major frontal columns as (re, im) pairs.
+int ref_dh_panel_front(void* h, const double* velocity, int p, int t, int* s, int* u, double* out) {
+    return Guard([&] {
+        const DH& H = *static_cast<DH*>(h);
+        if (p < 0 || p >= H.numPanels_) throw std::logic_error("no such panel");
+        const cliq::DistSymmInfo& info = H.PanelAnalysis(p);
+        if (t < 0 || t >= (int)info.localNodes.size()) throw std::logic_error("no such node");
+        *s = info.localNodes[t].size;
+        *u = (int)info.localNodes[t].lowerStruct.size();
+        if (!out) return;
+        const int nx = H.disc_.nx, ny = H.disc_.ny, nz = H.disc_.nz;
+        psp::DistUniformGrid<double> vel(nx, ny, nz, 0, 1);
+        std::copy(velocity, velocity + (size_t)nx * ny * nz, vel.Buffer());
+        const int vOffset = H.PanelV(p) - H.PanelPadding(p);
+        const int vSize = H.PanelDepth(p) + H.PanelPadding(p);
+        std::vector<double> myPanelVelocity;
+        std::vector<int> offsets;
+        std::map<int, int> nestedToNatural, naturalToNested;
+        H.GetPanelVelocity(vOffset, vSize, info, vel, myPanelVelocity, offsets, nestedToNatural, naturalToNested);
+        cliq::DistSymmFrontTree<Cd> fact;
+        H.FillPanelFronts(vOffset, vSize, info, fact, vel, myPanelVelocity, offsets, nestedToNatural,
+                          naturalToNested);
+        const elem::Matrix<Cd>& F = fact.localFronts[t].frontL;
+        Cd* o = reinterpret_cast<Cd*>(out);
+        for (int j = 0; j < F.Width(); ++j)
+            for (int i = 0; i < F.Height(); ++i) o[(size_t)j * F.Height() + i] = F.Get(i, j);
     });
 }
 

@@ -102,3 +102,29 @@ def test_global_rows_match_reference(name):
     assert A.nnz == B.nnz
     # the same formulas; the oracle's compiler may contract a multiply-add
     assert abs(A - B).max() <= 1e-14 * abs(B).max()
+
+
+@pytest.mark.parametrize("name", ["small", "dirichlet_top", "layered"])
+def test_panel_fronts_match_reference(name):
+    """Every node of every panel, as the reference's Initialize fills it
+    (GetPanelVelocity and FillPanelFronts with FormLowerColumnOfNode:
+    damped frequency, artificial PML below the panel, the panel's velocity
+    window), before any update: equal to the oracle's assembled fronts,
+    whose panel factorization the product's panel solves match."""
+    if name == "layered":
+        w = W.CONFIGS["layered_faults_24"]()
+    elif name == "dirichlet_top":
+        w = W.small_case(interior=(11, 9, 12), pml=4, freq=1.5, k=2, seed=11, top_pml=False)
+    else:
+        w = W.small_case()
+    d = w.disc
+    R = ref.RefHelmholtz(d)
+    O = oracle.Oracle(oracle.make_disc(d.omega, d.nx, d.ny, d.nz, d.wx, d.wy, d.wz,
+                                       bcs=(d.frontBC, d.rightBC, d.backBC, d.leftBC, d.topBC),
+                                       pml=(d.bx, d.by, d.bz), sigma=d.sigmax))
+    geo = O.geometry()
+    for p in range(geo.shape[0]):
+        for t in range(O.tree(geo[p, 3]).shape[0]):
+            a, b = R.panel_front(w.velocity, p, t), O.panel_front(w.velocity, p, t)
+            assert a.shape == b.shape, (p, t)
+            assert np.abs(a - b).max() <= 1e-14 * np.abs(b).max(), (p, t)
