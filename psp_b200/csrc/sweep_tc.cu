@@ -90,14 +90,15 @@ constexpr int kOutPerThread = kTcRows / kOutRowsPerPass;   // 16
 // Shapes of the kernels with NC right-hand sides per tile.
 //   B planes: 2 NC rows of B' (hi, then lo right after it).
 //   Accumulators: 4 NC f32 columns each ([A_hi B_hi + A_lo B_hi | A_hi B_lo]),
-//   kAccs of them (tiles in flight per CTA).
+//   kAccs of them (chains in flight per CTA), then the tile's chain sum
+//   (2 NC columns).
 //   Raw data of the stages in flight: A arrives by one tiled TMA copy per
 //   stage into a ring of RawSlots(fwd) slots shared by both groups (forward
 //   G's 128-row x 16-column box, [kc][row]; backward G^T's 128 x 16 box,
 //   [row][kc]); the forward keeps A in TMEM, so its last four slots reuse
 //   the A planes of the plane sets.  Each group has a ring of kOwn slots of
 //   its own copies of B (forward [plane][kc][n], backward [kc][n]), every
-//   entry read back by the thread that copied it.
+//   entry read back by the thread that copied it (OwnEntry).
 template <int NC>
 struct Cfg {
     static constexpr int kCols = NC;
