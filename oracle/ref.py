@@ -231,3 +231,17 @@ class RefHelmholtz:
         self._call(lib().ref_dh_panel_front, v.ctypes.data_as(ctypes.c_void_p), p, t, ctypes.byref(s),
                    ctypes.byref(u), out.ctypes.data_as(ctypes.c_void_p))
         return out.reshape(s.value, s.value + u.value).T
+
+    def apply(self, velocity, orc, B, op, panel=0):
+        """One of the reference's operators on a copy of B (natural order):
+        "multiply" (B := A B), "precondition" (the sweep around the
+        oracle's panel solves) or "panel" (SolvePanel of `panel`), each
+        between the reference's own pull and push of the right-hand
+        sides."""
+        v = np.ascontiguousarray(velocity, dtype=np.float64).reshape(-1)
+        X = np.ascontiguousarray(B, dtype=np.complex128).copy()
+        k = X.size // self.N
+        code = {"multiply": 0, "precondition": 1, "panel": 2}[op]
+        self._call(lib().ref_dh_apply, orc._h, v.ctypes.data_as(ctypes.c_void_p),
+                   X.ctypes.data_as(ctypes.c_void_p), k, code, panel)
+        return X

@@ -219,6 +219,50 @@ int ref_dh_solve(void* h, void* oracle, const double* velocity, double* grid, in
 
 const char* ref_dh_log() { return g_log.c_str(); }
 
+// One of the reference's operators on the k right-hand sides in `grid`
+// (natural order, interleaved), in place: op 0 Multiply (B := A B,
+// solve.hpp:613-679), op 1 Precondition (the sweep, 681-734, around the
+// oracle's panel solves), op 2 SolvePanel of panel `panel` alone
+// (736-882), each between the reference's own PullRightHandSides and
+// PushRightHandSides (58-239); the rows come from `velocity`.
+int ref_dh_apply(void* h, void* oracle, const double* velocity, double* grid, int k, int op, int panel) {
+    return Guard([&] {
+        DH& H = *static_cast<DH*>(h);
+        FormRows(H, velocity);
+        std::map<const void*, int> panelOf;
+        if ((int)H.fullInnerFacts_.size() != H.numFullInnerPanels_) {
+            H.fullInnerFacts_.clear();
+            for (int j = 0; j < H.numFullInnerPanels_; ++j)
+                H.fullInnerFacts_.push_back(new cliq::DistSymmFrontTree<Cd>);
+        }
+        for (int i = H.numPanels_ - 1; i >= 0; --i) panelOf[&H.PanelFactorization(i)] = i;
+        cliq::InstalledPanelSolver() = [&](const void* fact, cliq::DistNodalMultiVec<Cd>& X) {
+            OraclePanelSolve(H, oracle, panelOf.at(fact), X);
+        };
+        const int nx = H.disc_.nx, ny = H.disc_.ny, nz = H.disc_.nz;
+        psp::DistUniformGrid<Cd> G(nx, ny, nz, 0, k);
+        const size_t n = (size_t)nx * ny * nz * k;
+        std::copy(reinterpret_cast<const Cd*>(grid), reinterpret_cast<const Cd*>(grid) + n, G.Buffer());
+        elem::Matrix<Cd> B;
+        std::ostringstream log;
+        std::streambuf* old = std::cout.rdbuf(log.rdbuf());
+        try {
+            H.PullRightHandSides(G, B);
+            if (op == 0) H.Multiply(B);
+            else if (op == 1) H.Precondition(B);
+            else H.SolvePanel(B, panel);
+            H.PushRightHandSides(G, B);
+        } catch (...) {
+            std::cout.rdbuf(old);
+            cliq::InstalledPanelSolver() = nullptr;
+            throw;
+        }
+        std::cout.rdbuf(old);
+        cliq::InstalledPanelSolver() = nullptr;
+        std::copy(G.LockedBuffer(), G.LockedBuffer() + n, reinterpret_cast<Cd*>(grid));
+    });
+}
+
 // Global rows for a natural-order velocity: rowOffsets (N + 1 entries) and
 // the complex entries of every row (center, then the -x, +x, -y, +y, -v, +v
 // neighbours that exist), as Initialize forms them.  With entries null only

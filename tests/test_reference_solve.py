@@ -63,3 +63,21 @@ def test_reference_solve_restarts_like_oracle():
     assert sto["iterations"] > 5 and its == sto["iterations"]
     assert log.count("starting iteration") == -(-its // 5)
     assert rel(Xr, Xo) < 1e-12
+
+
+@pytest.mark.parametrize("name", list(CASES) + ["layered"])
+def test_reference_operators_match_oracle(name):
+    """Row by row of the scope table: the reference's own Multiply (A10),
+    Precondition (A9: panel solves with the sub- and superdiagonal
+    couplings, around the oracle's panel solves) and SolvePanel of every
+    panel (A8's data movement: node layout, padding rows), each between its
+    own PullRightHandSides and PushRightHandSides (A12), equal the oracle's
+    operators."""
+    w = _workload(name)
+    O = oracle_for(w.disc)
+    O.initialize(w.velocity)
+    R = ref.RefHelmholtz(w.disc)
+    assert rel(R.apply(w.velocity, O, w.rhs, "multiply"), O.multiply(w.rhs)) < 1e-14
+    assert rel(R.apply(w.velocity, O, w.rhs, "precondition"), O.precondition(w.rhs)) < 1e-13
+    for p in range(O.geometry().shape[0]):
+        assert rel(R.apply(w.velocity, O, w.rhs, "panel", p), O.solve_panel(w.rhs, p)) < 1e-14, p
