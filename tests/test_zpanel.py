@@ -140,7 +140,11 @@ def _thread_ranks(world, fn):
     return out
 
 
-def test_three_thread_ranks_sweep_and_solve_match_one_process():
+@pytest.mark.parametrize("blocks", [1, 2, 3])
+def test_three_thread_ranks_sweep_and_solve_match_one_process(blocks):
+    """blocks > 1: the sweep pipelined over blocks of right-hand-side
+    columns (a rank passes a block's boundary plane on and starts the next
+    block), which must not change any column's result."""
     import torch
     torch.set_num_threads(1)
     w = _case()
@@ -154,7 +158,7 @@ def test_three_thread_ranks_sweep_and_solve_match_one_process():
     def rank(r, comm):
         L = Ls[r]
         be = OracleSlabBackend(w, L, O)
-        S = Z.ZPanelSolver(L, be, comm, k)
+        S = Z.ZPanelSolver(L, be, comm, k, blocks=blocks)
         M = Z.scatter_slab(L, grid, k)
         S.precondition(M)
         X = Z.scatter_slab(L, grid, k)
@@ -170,7 +174,7 @@ def test_three_thread_ranks_sweep_and_solve_match_one_process():
     assert rel(X, Xo.reshape(ref.shape)) < 1e-9
 
 
-def _gloo_rank(rank, world, port, out_dir):
+def _gloo_rank(rank, world, port, out_dir, blocks=1):
     import torch
     import torch.distributed as dist
     from psp_b200 import ranks
@@ -184,7 +188,7 @@ def _gloo_rank(rank, world, port, out_dir):
         k, nxy = w.k, d.nx * d.ny
         grid = w.rhs.reshape(d.nz, nxy, k)
         L = _layouts(w, world)[rank]
-        S = Z.ZPanelSolver(L, OracleSlabBackend(w, L), Z.TorchComm(), k)
+        S = Z.ZPanelSolver(L, OracleSlabBackend(w, L), Z.TorchComm(), k, blocks=blocks)
         M = Z.scatter_slab(L, grid, k)
         S.precondition(M)
         X = Z.scatter_slab(L, grid, k)
@@ -201,11 +205,12 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def test_two_gloo_ranks_sweep_and_solve_match_one_process(tmp_path, monkeypatch):
+@pytest.mark.parametrize("blocks", [1, 2])
+def test_two_gloo_ranks_sweep_and_solve_match_one_process(tmp_path, monkeypatch, blocks):
     import torch.multiprocessing as mp
     for v in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
         monkeypatch.setenv(v, "1")
-    mp.spawn(_gloo_rank, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    mp.spawn(_gloo_rank, args=(2, _free_port(), str(tmp_path), blocks), nprocs=2, join=True)
     w = _case()
     d = w.disc
     O = oracle_for(d)
