@@ -874,6 +874,15 @@ int g_numSMs = 0;
 
 int GridFor(int n) { return n < g_numSMs ? n : g_numSMs; }
 
+// A CTA's tile count travels in the upper bits of a stage's packed place
+// (InfoSt: 11 bits for the tile, 10 each for the stage and the stage count).
+void CheckTilesPerCta(int n) {
+    const int g = GridFor(n);
+    if (g > 0 && (n + g - 1) / g >= (1 << 11))
+        throw PspError(kRuntimeError, "a sweep launch has more than 2047 tiles per CTA (" + std::to_string(n) +
+                                          " tiles); the problem is too large for one GPU's sweep tiling");
+}
+
 }  // namespace
 
 namespace {
@@ -921,6 +930,7 @@ void PrepareSweepTcKernels() {
 void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, int k, int cols,
                           const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
+    CheckTilesPerCta(n);
     if (cols == 32)
         LaunchPdl(sweep_tc_forward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles, n,
                   k, w);
@@ -933,6 +943,7 @@ void LaunchSweepForwardTc(const SweepFront<float>* fr, const SweepTile* tiles, i
 void LaunchSweepBackwardTc(const SweepFront<float>* fr, const SweepTile* tiles, int n, z64* B, int k, int cols,
                            const PanelIO& io, const SweepWork& w, cudaStream_t st) {
     if (n <= 0) return;
+    CheckTilesPerCta(n);
     if (cols == 32)
         LaunchPdl(sweep_tc_backward_kernel<32>, dim3(GridFor(n)), dim3(kTcThreads), Cfg<32>::kSmem, st, fr, tiles,
                   n, B, k, io, w);
