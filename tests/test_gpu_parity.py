@@ -77,8 +77,12 @@ def test_mixed_solve_reaches_tolerance(case):
     assert rel(Xm, X) < 1e-4
 
 
-def test_golden_fixture(product_lib):
-    path = os.path.join(os.path.dirname(__file__), "golden", "small_fp64.npz")
+@pytest.mark.parametrize("name", ["small_fp64.npz", "reference_dirichlet_top.npz"])
+def test_golden_fixture(product_lib, name):
+    """small_fp64: written by the oracle; reference_dirichlet_top: written
+    by the reference's own Multiply, Precondition and Solve (around the
+    oracle's panel solves), 55 GMRES(20) steps over three restart cycles."""
+    path = os.path.join(os.path.dirname(__file__), "golden", name)
     g = np.load(path)
     cfg = {k: g["cfg_" + k] for k in ("interior", "pml", "freq", "k", "seed", "top_pml")}
     w = W.small_case(interior=tuple(int(v) for v in cfg["interior"]), pml=int(cfg["pml"]),
@@ -86,6 +90,8 @@ def test_golden_fixture(product_lib):
                      top_pml=bool(cfg["top_pml"]))
     H = P.DistHelmholtz(w.disc)
     H.Initialize(g["velocity"], precision=P.FP64)
+    if "multiply" in g.files:
+        assert rel(H.multiply(g["rhs"]), g["multiply"]) < 1e-13
     assert rel(H.precondition(g["rhs"]), g["precondition"]) < 1e-12
     X = g["rhs"].copy()
     st = H.Solve(X, 20, float(g["rel_tol"]))
