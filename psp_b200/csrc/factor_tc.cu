@@ -80,6 +80,7 @@ static_assert(kConvThreads == 2 * kBM && kConvThreads == 4 * kBN, "converter thr
 struct Sync {
     uint64_t planeFull[kPlaneSets], planeEmpty[kPlaneSets];
     uint64_t accFull[kAccs], accEmpty[kAccs];
+    uint64_t mmaDrain;           // the MMA thread's last commit when a role gave up
     int rawFlags[kRaw];          // written and read by converter thread 0
     int planeFlags[kPlaneSets];  // converter thread 0 -> MMA thread
     uint32_t tmem;
@@ -415,6 +416,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
             umma::MbarInit(&S.accFull[i], 1);
             umma::MbarInit(&S.accEmpty[i], kEpiThreads);
         }
+        umma::MbarInit(&S.mmaDrain, 1);
         S.abort = 0;
         umma::FenceMbarInit();
     }
@@ -431,6 +433,18 @@ __global__ void __launch_bounds__(kFThreads, 1)
     }
     umma::FenceBeforeSync();
     __syncthreads();
+    // when a role gave up, the MMA thread waits (bounded) for the tensor-core
+    // operations it issued before tensor memory is freed (S.abort is no
+    // longer written, so every thread takes the same branch; the converters
+    // have waited for their own copies)
+    if (*reinterpret_cast<volatile int*>(&S.abort)) {
+        if (tid == kMma0) {
+            umma::CommitTo(&S.mmaDrain);
+            umma::MbarWaitBounded(&S.mmaDrain, 0, nullptr);
+        }
+        umma::FenceBeforeSync();
+        __syncthreads();
+    }
     if (tid / 32 == 0) {
         umma::FenceAfterSync();
         umma::TmemDealloc(S.tmem, kTmemCols);

@@ -157,12 +157,14 @@ struct Sync {
     uint64_t planeFull[kPlaneSets], planeEmpty[kPlaneSets];
     uint64_t accFull[kAccMax], accEmpty[kAccMax];
     uint64_t rawFull[kRawMax], rawEmpty[kRawMax];
+    uint64_t mmaDrain;           // the MMA thread's last commit when a role gave up
     StageHdr hdr[kPlaneSets];
     int ownInfo[kGroups][kOwnMax];  // stage place, packed (see InfoSt); written and read by a group's first thread
     int rawK[kRawMax][2];        // stage's first K index and the tile's K end
     uint32_t tmem;
     int abort;
     int isLast;
+    int rawIssued;  // raw A copies the producer issued
 };
 
 // Bounded wait (umma::kWaitLimitNs); false once this or another role gave up.
@@ -316,9 +318,10 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
     if ((threadIdx.x & 31) != 0) return;
     LoadCursor<kFwd> cur;
     cur.Start(fr, tiles, n, k);
-    for (int g = 0; cur.Valid(g); ++g) {
+    int g = 0;
+    for (; cur.Valid(g); ++g) {
         const int slot = g % C::RawSlots(kFwd);
-        if (g >= C::RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / C::RawSlots(kFwd)) - 1) & 1, S, status)) return;
+        if (g >= C::RawSlots(kFwd) && !Wait(&S.rawEmpty[slot], ((g / C::RawSlots(kFwd)) - 1) & 1, S, status)) break;
         const LoadMeta& m = cur.m;
         const int kBase = cur.KBase();
         S.rawK[slot][0] = kBase;
@@ -331,6 +334,17 @@ __device__ void ProducerRole(const SweepFront<float>* __restrict__ fr, const Swe
             umma::TmaLoad2D(RawSlotPtr<NC, kFwd>(smem, slot), map, kBase, m.row0, &S.rawFull[slot]);
         cur.Advance();
     }
+    S.rawIssued = g;
+}
+
+// After a role gave up: waits (bounded) until the last copy into every raw
+// slot has landed, so none is in flight when the CTA exits.  Copy g of the
+// ring fills slot g % R in its phase g / R.
+template <int NC, bool kFwd>
+__device__ __forceinline__ void DrainRaw(Sync& S) {
+    constexpr int R = Cfg<NC>::RawSlots(kFwd);
+    const int G = S.rawIssued;
+    for (int s = 0; s < R && s < G; ++s) umma::MbarWaitBounded(&S.rawFull[s], ((G - 1 - s) / R) & 1, nullptr);
 }
 
 // ------------------------------------------------------------------ converters
@@ -802,7 +816,9 @@ __device__ __forceinline__ void InitSync(Sync& S) {
             umma::MbarInit(&S.rawFull[i], 1);
             umma::MbarInit(&S.rawEmpty[i], kGroupThreads);
         }
+        umma::MbarInit(&S.mmaDrain, 1);
         S.abort = 0;
+        S.rawIssued = 0;
         umma::FenceMbarInit();
     }
     if (threadIdx.x / 32 == 0) umma::TmemAlloc(&S.tmem, kTmemCols);
@@ -811,9 +827,24 @@ __device__ __forceinline__ void InitSync(Sync& S) {
     umma::FenceAfterSync();
 }
 
+// Every role has returned.  When one gave up, the others may have left
+// asynchronous work behind: the MMA thread waits (bounded) for its
+// tensor-core operations, the producer for its copies, before the CTA frees
+// tensor memory and exits.  S.abort is no longer written, so every thread
+// takes the same branch.
+template <int NC, bool kFwd>
 __device__ __forceinline__ void Teardown(Sync& S) {
     umma::FenceBeforeSync();
     __syncthreads();
+    if (*reinterpret_cast<volatile int*>(&S.abort)) {
+        if (threadIdx.x == kMma0) {
+            umma::CommitTo(&S.mmaDrain);
+            umma::MbarWaitBounded(&S.mmaDrain, 0, nullptr);
+        }
+        if (threadIdx.x == kProd0) DrainRaw<NC, kFwd>(S);
+        umma::FenceBeforeSync();
+        __syncthreads();
+    }
     if (threadIdx.x / 32 == 0) {
         umma::FenceAfterSync();
         umma::TmemDealloc(S.tmem, kTmemCols);
@@ -844,7 +875,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_forward_kernel(const S
     } else if (tid >= kProd0) {
         ProducerRole<NC, true>(fr, tiles, n, k, smem, S, work.status);
     }
-    Teardown(S);
+    Teardown<NC, true>(S);
 }
 
 template <int NC>
@@ -867,7 +898,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) sweep_tc_backward_kernel(const 
     } else if (tid >= kProd0) {
         ProducerRole<NC, false>(fr, tiles, n, k, smem, S, work.status);
     }
-    Teardown(S);
+    Teardown<NC, false>(S);
 }
 
 int g_numSMs = 0;
