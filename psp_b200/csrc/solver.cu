@@ -920,12 +920,21 @@ typename FactorStore<R>::SolvePlan& FactorStore<R>::Plan(int k) {
     // nothing extra and save split-K partial sums) and only shrinks to give
     // every SM tiles; `forceChunk` > 0 fixes it instead (tuning candidates).
     int64_t maxPartialRows = kTcRows, maxCounters = 1;
-    // Longest K-chunk of a tensor-core tile (PSP_B200_SWEEP_TC_MAX_CHUNK, a
-    // power of two from 16 to 512), and a fixed chunk for the default
-    // tensor-core tiling in place of the shrinking rule below
-    // (PSP_B200_SWEEP_TC_CHUNK, tests).
-    const int tcMaxChunk = (int)std::max(16LL, std::min(512LL, EnvInt("PSP_B200_SWEEP_TC_MAX_CHUNK", 512)));
-    const int tcFixedChunk = (int)std::max(0LL, std::min((long long)tcMaxChunk, EnvInt("PSP_B200_SWEEP_TC_CHUNK", 0)));
+    // Longest K-chunk of a tensor-core tile (PSP_B200_SWEEP_TC_MAX_CHUNK),
+    // and a fixed chunk for the default tensor-core tiling in place of the
+    // shrinking rule below (PSP_B200_SWEEP_TC_CHUNK, tests; 0 = unset).
+    // Both are rounded down to a power of two from 16 to 512: a backward
+    // tile's K start is the innermost coordinate of its TMA copies, which
+    // must be even (16-byte aligned complex-single entries), and chunks of
+    // whole stages keep it so.
+    auto chunkSetting = [](long long v) {
+        int c = 16;
+        while (2LL * c <= std::min(v, 512LL)) c *= 2;
+        return c;
+    };
+    const int tcMaxChunk = chunkSetting(EnvInt("PSP_B200_SWEEP_TC_MAX_CHUNK", 512));
+    const long long tcChunkEnv = EnvInt("PSP_B200_SWEEP_TC_CHUNK", 0);
+    const int tcFixedChunk = tcChunkEnv > 0 ? std::min(tcMaxChunk, chunkSetting(tcChunkEnv)) : 0;
     auto makeTiles = [&](const ClassStructure& cs, int d, bool fwd, bool tcTiles, int cols, int forceChunk,
                          std::vector<SweepTile>& tiles) {
         const int maxChunk = tcTiles ? tcMaxChunk : SweepMaxChunk<R>();
