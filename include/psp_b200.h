@@ -161,12 +161,16 @@ int psp_cu_solve_panel(psp_cu_handle* h, double* B, int k, int panel);
  * on a device slab, in place.  in_mode 0: B_i := T_i B_i; 1: B_i := T_i (B_i
  * - A_{i,i-1} B_{i-1}), reading the plane below the panel; 2: B_i := T_i
  * (-A_{i,i+1} B_{i+1}), reading the plane above it; out_accumulate adds the
- * result to B_i instead of replacing it.
+ * result to B_i instead of replacing it.  The slab must hold every plane the
+ * solve touches: a z_base above the lowest one, or an in_mode whose
+ * neighbouring panel does not exist, is a logic error; the caller makes the
+ * slab reach the highest one (the library is not told the slab's length).
  *
  * psp_cu_multiply_slab: Y := A X, or Y := Bv - A X when Bv is not NULL, on
  * planes [z_first, z_first + z_count) of device slabs X, Y, Bv whose first
  * stored plane is z_slab; X must hold the planes next to that range that
- * exist in the grid (the halo). */
+ * exist in the grid (the halo): a z_slab above z_first - 1 is a logic error,
+ * and the caller makes the slabs reach plane z_first + z_count. */
 int psp_cu_set_panel_range(psp_cu_handle* h, int p0, int p1);
 int psp_cu_solve_panel_slab(psp_cu_handle* h, double* d_B, int k, int panel, int in_mode, int out_accumulate,
                             int z_base);

@@ -356,6 +356,7 @@ def interpolate_grid(grid, old_sizes, new_sizes, numScalars=1):
     if src.numel() != nx0 * ny0 * nz0 * numScalars:
         raise LogicError("grid size does not match its dimensions")
     is_complex = src.is_complex()
+    _device_tensor(src, "grid", "complex128" if is_complex else "float64", src.device.index)
     out = torch.empty((nz, ny, nx, numScalars), dtype=src.dtype, device=src.device)
     with torch.cuda.device(src.device):
         torch.cuda.synchronize()
@@ -379,8 +380,10 @@ class DistHelmholtz:
         _check(lib().psp_cu_create(ctypes.byref(self._d), float(damping), int(numPlanesPerPanel), int(cutoff),
                                    int(device), ctypes.byref(h)))
         self._h = h
+        self.device = int(device)
         self.N = disc.nx * disc.ny * disc.nz
         self.last_stats = None
+        self._geometry = None
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -408,6 +411,7 @@ class DistHelmholtz:
             if velocity.numel() != self.N:
                 raise LogicError("Velocity grid is incorrect")
             v = velocity.contiguous()
+            _device_tensor(v, "velocity", "float64", self.device, numel=self.N)
             _check(lib().psp_cu_initialize_device(self._h, ctypes.c_void_p(v.data_ptr()), panelScheme, precision))
             self.factor_version = getattr(self, "factor_version", 0) + 1
             return
@@ -435,7 +439,7 @@ class DistHelmholtz:
 
     def _solve(self, B, m, relTol):
         if _is_cuda_tensor(B):
-            k = B.numel() // self.N
+            k = _device_tensor(B, "B", "complex128", self.device, per=self.N)
             st = _Stats()
             _check(lib().psp_cu_solve_device(self._h, ctypes.c_void_p(B.data_ptr()), k, m, relTol,
                                              ctypes.byref(st)))
@@ -502,6 +506,8 @@ class DistHelmholtz:
     def _grid_op(self, fn, B, *extra):
         X = np.ascontiguousarray(B, dtype=np.complex128).copy()
         k = X.size // self.N
+        if k == 0 or k * self.N != X.size:
+            raise LogicError("B does not match the grid")
         _check(fn(self._h, _dptr(X.view(np.float64)), k, *extra))
         return X
 
@@ -550,30 +556,67 @@ class DistHelmholtz:
         first Initialize."""
         _check(lib().psp_cu_set_panel_range(self._h, int(p0), int(p1)))
 
+    def _panel_planes(self, panel, in_mode):
+        """(lowest, highest) grid plane z that SolvePanel of `panel` reads or
+        writes: its own planes, and the plane below (in_mode 1) or above
+        (in_mode 2) it."""
+        if self._geometry is None:
+            self._geometry = self.geometry()
+        if not 0 <= panel < self._geometry.shape[0]:
+            raise LogicError("panel index out of range")
+        low_v, depth = int(self._geometry[panel, 0]), int(self._geometry[panel, 1])
+        nz = self.disc.nz
+        z_lo, z_hi = nz - 1 - (low_v + depth - 1), nz - 1 - low_v
+        if in_mode == 2:
+            z_lo -= 1
+        elif in_mode == 1:
+            z_hi += 1
+        if z_lo < 0 or z_hi > nz - 1:
+            raise LogicError("panel %d has no neighbouring panel for in_mode %d" % (panel, in_mode))
+        return z_lo, z_hi
+
     def solve_panel_slab(self, B, k, panel, in_mode, out_accumulate, z_base):
         """SolvePanel on a CUDA complex128 slab of planes z_base.. (in place)."""
+        nxy = self.disc.nx * self.disc.ny
+        planes = _device_tensor(B, "B", "complex128", self.device, per=nxy * int(k))
+        z_lo, z_hi = self._panel_planes(int(panel), int(in_mode))
+        if z_base > z_lo or z_base + planes - 1 < z_hi:
+            raise LogicError("the slab (planes %d..%d) must hold planes %d..%d of panel %d"
+                             % (z_base, z_base + planes - 1, z_lo, z_hi, panel))
         _check(lib().psp_cu_solve_panel_slab(self._h, ctypes.c_void_p(B.data_ptr()), int(k), int(panel),
                                              int(in_mode), int(out_accumulate), int(z_base)))
 
     def multiply_slab(self, X, Y, k, z_first, z_count, z_slab, Bv=None):
         """Y := A X (or Bv - A X) on planes [z_first, z_first + z_count) of
         CUDA complex128 slabs whose first stored plane is z_slab."""
+        nxy, nz = self.disc.nx * self.disc.ny, self.disc.nz
+        planes = _device_tensor(X, "X", "complex128", self.device, per=nxy * int(k))
+        for t, name in ((Y, "Y"), (Bv, "Bv")):
+            if t is not None and _device_tensor(t, name, "complex128", self.device, per=nxy * int(k)) != planes:
+                raise LogicError("%s must be a slab of the same planes as X" % name)
+        z_lo, z_hi = max(0, z_first - 1), min(nz - 1, z_first + z_count)  # with the halo planes
+        if z_count < 1 or z_slab > z_lo or z_slab + planes - 1 < z_hi:
+            raise LogicError("the slabs (planes %d..%d) must hold planes %d..%d"
+                             % (z_slab, z_slab + planes - 1, z_lo, z_hi))
         _check(lib().psp_cu_multiply_slab(self._h, ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(Y.data_ptr()),
                                           ctypes.c_void_p(Bv.data_ptr()) if Bv is not None else None, int(k),
                                           int(z_first), int(z_count), int(z_slab)))
 
     def multiply_device(self, B):
-        _check(lib().psp_cu_multiply_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+        k = _device_tensor(B, "B", "complex128", self.device, per=self.N)
+        _check(lib().psp_cu_multiply_device(self._h, ctypes.c_void_p(B.data_ptr()), k))
 
     def multiply_device_noalloc(self, B):
         """B := A B in place on a CUDA tensor without any device allocation
         (for callers inside their own stream capture, or with a fixed memory
         reservation); nx*ny*nz*k must not exceed 1048576, and calls that
         overlap on the GPU race on the shared scratch array."""
-        _check(lib().psp_cu_multiply_device_noalloc(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+        k = _device_tensor(B, "B", "complex128", self.device, per=self.N)
+        _check(lib().psp_cu_multiply_device_noalloc(self._h, ctypes.c_void_p(B.data_ptr()), k))
 
     def precondition_device(self, B):
-        _check(lib().psp_cu_precondition_device(self._h, ctypes.c_void_p(B.data_ptr()), B.numel() // self.N))
+        k = _device_tensor(B, "B", "complex128", self.device, per=self.N)
+        _check(lib().psp_cu_precondition_device(self._h, ctypes.c_void_p(B.data_ptr()), k))
 
     def gradient_device(self, U, Z, grad=None, accumulate=False):
         """Velocity gradient -Re(dA_ii/dvel_i * sum_r Z[i,r] U[i,r]) of a real
@@ -581,13 +624,14 @@ class DistHelmholtz:
         tensors of nx*ny*nz*k entries, natural order); returns (or adds to)
         a CUDA float64 tensor of nx*ny*nz entries."""
         import torch
-        k = U.numel() // self.N
-        if U.numel() != Z.numel() or k * self.N != U.numel():
+        U, Z = U.contiguous(), Z.contiguous()
+        k = _device_tensor(U, "U", "complex128", self.device, per=self.N)
+        if _device_tensor(Z, "Z", "complex128", self.device, per=self.N) != k:
             raise LogicError("U and Z must be grids of the same k right-hand sides")
         if grad is None:
             grad = torch.zeros(self.N, dtype=torch.float64, device=U.device)
             accumulate = False
-        U, Z = U.contiguous(), Z.contiguous()
+        _device_tensor(grad, "grad", "float64", self.device, numel=self.N)
         _check(lib().psp_cu_gradient_device(self._h, ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(Z.data_ptr()), k,
                                             ctypes.c_void_p(grad.data_ptr()), 1 if accumulate else 0))
         return grad
@@ -636,3 +680,28 @@ def _stats_dict(st):
 
 def _is_cuda_tensor(x):
     return getattr(x, "is_cuda", False) and hasattr(x, "data_ptr")
+
+
+def _device_tensor(t, what, dtype, device, per=None, numel=None):
+    """Checks a CUDA tensor before its pointer crosses the C ABI, which sees
+    only an address and a count: another dtype, a strided view, a size that
+    is not a whole number of grids or a tensor on another GPU would make the
+    kernels read or write outside it.  Returns numel // per (or numel)."""
+    import torch
+    want = getattr(torch, dtype)
+    if t.dtype != want:
+        raise LogicError("%s must be a %s tensor, not %s" % (what, dtype, str(t.dtype).replace("torch.", "")))
+    if not t.is_contiguous():
+        raise LogicError("%s must be contiguous" % what)
+    if t.is_conj() or t.is_neg():
+        raise LogicError("%s is a lazily conjugated or negated view: resolve it first" % what)
+    if t.device.index != device:
+        raise LogicError("%s is on cuda:%s but the handle runs on cuda:%d" % (what, t.device.index, device))
+    n = t.numel()
+    if numel is not None and n != numel:
+        raise LogicError("%s must hold %d entries, not %d" % (what, numel, n))
+    if per is not None:
+        if n == 0 or n % per:
+            raise LogicError("%s must hold a positive multiple of %d entries, not %d" % (what, per, n))
+        return n // per
+    return n

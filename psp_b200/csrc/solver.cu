@@ -1615,6 +1615,17 @@ void Helmholtz::SolvePanelSlab(z64* B, int k, int panel, int inMode, int outAccu
     if (panel < 0 || panel >= an_.geom.numPanels) throw PspError(kLogicError, "panel index out of range");
     if (inMode < 0 || inMode > 2 || k < 1 || zBase < 0 || zBase >= an_.disc.nz)
         throw PspError(kLogicError, "invalid panel-solve arguments");
+    // the lowest plane the panel solve touches: its top plane, or the plane
+    // above it whose coupling in_mode 2 reads; in_mode 1 reads the plane
+    // below its bottom one
+    const PanelGeometry& g = an_.geom;
+    const int zLow = an_.disc.nz - 1 - (g.LowV(panel) + g.Depth(panel) - 1) - (inMode == 2 ? 1 : 0);
+    if (zLow < 0 || (inMode == 1 && g.LowV(panel) == 0))
+        throw PspError(kLogicError, "panel " + std::to_string(panel) + " has no neighbouring panel for in_mode " +
+                                        std::to_string(inMode));
+    if (zBase > zLow)
+        throw PspError(kLogicError, "the slab starts at plane " + std::to_string(zBase) + ", above plane " +
+                                        std::to_string(zLow) + " that panel " + std::to_string(panel) + " needs");
     CUDA_CHECK(cudaSetDevice(device_));
     ProfilerBinding bind(&prof_);
     const int w = RhsBlockWidth(k);
@@ -1629,7 +1640,10 @@ void Helmholtz::SolvePanelSlab(z64* B, int k, int panel, int inMode, int outAccu
 
 void Helmholtz::MultiplySlab(const z64* X, z64* Y, const z64* Bv, int k, int zFirst, int zCount, int zSlab) {
     if (!dVel_.p) throw PspError(kNotInitialized, "DistHelmholtz is not initialized");
-    if (k < 1 || zCount < 1 || zFirst < 0 || zFirst + zCount > an_.disc.nz || zSlab > zFirst || zSlab < 0)
+    // the slab must begin at or below the halo plane zFirst - 1 (which the
+    // stencil of plane zFirst reads when it exists)
+    if (k < 1 || zCount < 1 || zFirst < 0 || zFirst + zCount > an_.disc.nz || zSlab < 0 ||
+        zSlab > std::max(0, zFirst - 1))
         throw PspError(kLogicError, "invalid slab multiply arguments");
     CUDA_CHECK(cudaSetDevice(device_));
     LaunchHelmholtzApplyPlanes(X, Y, Bv, dVel_.as<double>(), sp_, k, zFirst, zCount, zSlab, stream_);
