@@ -74,6 +74,12 @@ void OnDeviceCopy(psp_cu_handle* h, double* B, int k, F&& fn) {
     h->io.ToHost(B, d, bytes, s->stream());
 }
 
+// A device grid argument: a pointer and at least one right-hand side.
+void CheckDeviceGrid(const void* d, int k) {
+    if (!d) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
+    if (k < 1) throw PspError(PSP_CU_LOGIC_ERROR, "need at least one right-hand side");
+}
+
 }  // namespace
 
 namespace psp_b200 {
@@ -169,7 +175,7 @@ int psp_cu_solve(psp_cu_handle* h, double* B, int k, int m, double rel_tol, psp_
 int psp_cu_solve_device(psp_cu_handle* h, double* d_B, int k, int m, double rel_tol, psp_cu_stats* stats) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {
-        if (!d_B) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
+        CheckDeviceGrid(d_B, k);
         psp_b200::SolveStats s;
         h->solver->SolveDevice(reinterpret_cast<psp_b200::z64*>(d_B), k, m, rel_tol, &s);
         FillStats(s, stats);
@@ -198,18 +204,25 @@ int psp_cu_precondition(psp_cu_handle* h, double* B, int k) {
 
 int psp_cu_multiply_device(psp_cu_handle* h, double* d_B, int k) {
     if (int e = CheckHandle(h)) return e;
-    return Guard([&] { h->solver->MultiplyDevice(reinterpret_cast<psp_b200::z64*>(d_B), k); });
+    return Guard([&] {
+        CheckDeviceGrid(d_B, k);
+        h->solver->MultiplyDevice(reinterpret_cast<psp_b200::z64*>(d_B), k);
+    });
 }
 
 int psp_cu_precondition_device(psp_cu_handle* h, double* d_B, int k) {
     if (int e = CheckHandle(h)) return e;
-    return Guard([&] { h->solver->PreconditionDevice(reinterpret_cast<psp_b200::z64*>(d_B), k); });
+    return Guard([&] {
+        CheckDeviceGrid(d_B, k);
+        h->solver->PreconditionDevice(reinterpret_cast<psp_b200::z64*>(d_B), k);
+    });
 }
 
 int psp_cu_gradient_device(psp_cu_handle* h, const double* d_U, const double* d_Z, int k, double* d_grad,
                            int accumulate) {
     if (int e = CheckHandle(h)) return e;
     return Guard([&] {
+        if (!d_U || !d_Z || !d_grad) throw PspError(PSP_CU_LOGIC_ERROR, "null grid");
         h->solver->GradientDevice(reinterpret_cast<const psp_b200::z64*>(d_U),
                                   reinterpret_cast<const psp_b200::z64*>(d_Z), k, d_grad, accumulate != 0);
     });
